@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""Benchmark of the MCV_SW explicit RK step on B200.
+
+`python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]`
+
+One step = one RK step (all stages + halo corrections) of the workload on every
+GPU.  Default workload: MCV4, Nc=256, RK3_TVD, seeded balanced tilted zonal flow
++ spherical-harmonic height perturbation (degree <= 32, RMS 20 m) + a 2000 m
+Gaussian mountain (the single-large-instance configuration).  The state stays
+resident in HBM; `value` is simulated days per wall second over all GPUs
+(replicas: every rank advances its own instance).  Each stage reads ~9 padded
+FP64 fields (~260 MB) -- more than the 126 MB L2 -- so no L2 flush is needed.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+FP64 C restatement under oracle/, all host threads) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sim-days/s MCV4 Nc=256 mixed vs FP64 on 1 B200 at stated L2 error; p99 latency"
+UNIT = "sim-days/s"
+DEFAULT_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["large", "small", "stress"], default="large")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=5)
+    return p.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_workload(name):
+    from mcv_sw_b200 import cases
+    if name == "large":
+        st, geom = cases.large(seed=2)
+        desc = "MCV4 Nc=256 RK3_TVD, seeded balanced tilted zonal flow + harmonics (deg<=32, RMS 20 m) + 2000 m mountain"
+    elif name == "small":
+        st, geom = cases.small(seed=1)
+        desc = "MCV3 Nc=32 RK4, seeded balanced tilted zonal flow + harmonics (deg 1-8, RMS 10 m)"
+    else:
+        st, geom = cases.stress(seed=5)
+        desc = "MCV4 Nc=1024 RK4, balanced zonal flow + Rossby-Haurwitz waves R=4..12 (50-200 m)"
+    return st, geom, desc
+
+
+def stage_words(scheme, precision):
+    """Algorithmic 8-byte words per interior PV per stage: stage input (3),
+    RK base where the stage reads it (3), 6 metric scalars, stage output (3),
+    RK4 accumulator read/write (3 each)."""
+    if scheme == "RK3_TVD":
+        return [12, 15, 15]
+    return [15, 21, 21, 18]
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return DEFAULT_HBM_GBS, "fallback"
+
+
+def stage_traffic_per_pv():
+    """DRAM bytes per interior PV per stage-kernel launch from the committed ncu
+    summary (profiles/stage_kernel_traffic.txt: `<workload> <kind> <bytes_per_pv>`)."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            parts = line.split()
+            if len(parts) == 3 and not line.startswith("#"):
+                out[(parts[0], parts[1])] = float(parts[2])
+    return out
+
+
+def cpu_baseline(st, budget_s=20.0):
+    """The oracle (FP64 C restatement, all host threads) on a bounded sample of
+    the same workload: as many RK steps as fit in ~budget_s."""
+    from oracle import oracle as orc
+    o = orc.Oracle(st.order, st.nc, st.dt, st.scheme, 6.371e6)
+    o.set_phi_s(st.phi_s)
+    o.init_state(st.zonal, st.merid, st.phi)
+    t0 = time.perf_counter()
+    o.step(1)
+    t1 = time.perf_counter() - t0
+    nsteps = max(1, min(200, int(budget_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    o.step(nsteps)
+    el = time.perf_counter() - t0
+    return {"value": nsteps * st.dt / 86400.0 / el, "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
+            "sample": f"{nsteps} RK steps of the same workload after 1 warm-up step ({el:.1f} s)"}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    st, geom, desc = build_workload(args.workload)
+    from oracle import oracle as orc
+    o = orc.Oracle(st.order, st.nc, st.dt, st.scheme, 6.371e6)
+    o.set_phi_s(st.phi_s)
+    o.init_state(st.zonal, st.merid, st.phi)
+    o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    el = time.perf_counter() - t0
+    value = args.steps * st.dt / 86400.0 / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": desc, "order": st.order, "nc": st.nc, "scheme": st.scheme,
+                                            "precision": "fp64", "dt_s": st.dt},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
+                             "sample": f"{args.steps} RK steps after {args.warmup} warm-up steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from mcv_sw_b200 import api
+    st, geom, desc = build_workload(args.workload)
+    n_pv = 6 * geom.n * geom.n
+
+    s = api.Stepper(st.order, st.nc, st.dt, st.scheme, members=1, precision=args.precision,
+                    radius=6.371e6)
+    s.set_geometry(geom)
+    s.set_member(0, st.phi_s, st.u, st.v, st.phi)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    s.time_steps(max(args.warmup, 3))
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = s.time_steps(args.steps)
+    barrier()
+    clk = clocks.stop()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    sim_days = args.steps * st.dt / 86400.0
+    value = world * sim_days / (ms / 1e3)
+
+    # roofline of the fused stage kernel: algorithmic bytes / launch time
+    stage_ms, halo_ms = s.profile_step(3)
+    words = stage_words(st.scheme, args.precision)
+    alg_bytes = [w * 8 * n_pv for w in words]
+    achieved = sum(alg_bytes) / (sum(stage_ms) * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic_pv = stage_traffic_per_pv()
+    key = (args.workload, f"{st.scheme}-{args.precision}")
+    traffic = traffic_pv[key] * n_pv if key in traffic_pv else None
+    step_ms = ms / args.steps
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind, "kernel": "stage_kernel",
+                "algorithmic_bytes_per_launch": sum(alg_bytes) / len(alg_bytes),
+                "stage_ms": stage_ms, "halo_ms": halo_ms,
+                "halo_share_of_step": len(stage_ms) * halo_ms / step_ms}
+
+    # end to end through the C ABI with pinned host buffers: per step upload the
+    # state, advance one RK step, download the state
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hp = {k: pin(getattr(st, k)) for k in ("phi_s", "u", "v", "phi")}
+    ho = {k: torch.empty(geom.shape, dtype=torch.float64).pin_memory().numpy() for k in ("u", "v", "phi")}
+    s.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
+    s.step(1)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        s.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
+        s.step(1)
+        s.get_state(0, out=ho)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    field_bytes = 8 * 6 * geom.npx * geom.npx
+    e2e = {"value": world * args.e2e_steps * st.dt / 86400.0 / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 4 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
+           "how": "per step: mcv_set_member (phi_s, u, v, phi from pinned host) + mcv_step(1) + "
+                  "mcv_get_state (u, v, phi to pinned host); host wall clock around synchronous calls"}
+    s.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(st)
+    if rank == 0:
+        stages = len(words)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+                "config": {"workload": desc, "order": st.order, "nc": st.nc, "scheme": st.scheme,
+                           "precision": args.precision, "dt_s": st.dt, "interior_pvs": n_pv,
+                           "parallelism": f"replicas{world}",
+                           "l2": "no flush: each stage reads > 126 MB (inputs larger than L2)"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": args.steps * 2 * stages, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

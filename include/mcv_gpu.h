@@ -1,0 +1,165 @@
+/*
+ * mcv_gpu.h -- C ABI of the B200 implementation of MCV_SW's explicit RK step.
+ *
+ * The reference has no FFI: its time loop calls the Fortran subroutines
+ *   RK4(stat(new), stat(old))       src/time_scheme_mod.F90:13-44
+ *   RK3_TVD(stat(new), stat(old))   src/time_scheme_mod.F90:46-69
+ * from src/MCV_SW.F90:57-60, on module-global arrays.  This header is the
+ * drop-in boundary for that loop: a Fortran driver binds it with
+ * iso_c_binding, Python binds it with ctypes.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 = OK, < 0 = error;
+ *    mcv_last_error() returns a message for the last failing call on the
+ *    calling thread.
+ *  - Host arrays are FP64 (or int32) in the reference's Fortran layout:
+ *    column-major (i, j, panel) over the padded point range
+ *    i, j = ips..ipe (npx = nPVx + 2*nPVHalo points per direction), 6 panels;
+ *    2x2 matrices are (2, 2, i, j, panel).  The library copies host arrays;
+ *    it never keeps a host pointer.
+ *  - A handle owns one CUDA stream and all device memory of one grid
+ *    (order, Nc) with `members` independent states.  A handle is not
+ *    thread-safe; different handles are independent.
+ *  - There is no CPU fallback: without a usable sm_100 GPU, mcv_create fails.
+ */
+#ifndef MCV_GPU_H
+#define MCV_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mcv_handle mcv_handle;
+
+/* integral_scheme (src/parameters_mod.F90:228-235) */
+#define MCV_RK3_TVD 3
+#define MCV_RK4 4
+/* arithmetic of the step */
+#define MCV_FP64 0  /* FP64 throughout (the plain form)                      */
+#define MCV_MIXED 1 /* FP32 tendencies on phi - mean, FP64 state accumulation */
+
+/* status codes */
+#define MCV_OK 0
+#define MCV_ERR_ARG (-1)       /* invalid argument or size                   */
+#define MCV_ERR_CUDA (-2)      /* CUDA runtime error / no usable GPU         */
+#define MCV_ERR_NOMEM (-3)     /* device allocation failed                   */
+#define MCV_ERR_ORDER (-4)     /* call order (e.g. step before geometry)     */
+#define MCV_ERR_NONFINITE (-5) /* a member's state became NaN/Inf            */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *mcv_last_error(void);
+
+/* ---------------------------------------------------------------------
+ * Core stepping API: replaces the RK4 / RK3_TVD calls of the time loop.
+ * ------------------------------------------------------------------- */
+
+/* Allocate a handle for `members` states on one grid.
+ * Replaces initParameters / initStat / initTend (src/parameters_mod.F90:134-239,
+ * src/stat_mod.F90:25-45, src/tend_mod.F90:17-28).  nc = 90/dx (cells per
+ * panel edge), order = DOF (3 = MCV3, 4 = MCV4, src/constants_mod.F90:4-10),
+ * dt in seconds; radius only documents the geometry passed to
+ * mcv_set_geometry (it is not used by the step itself). */
+int mcv_create(int order, int nc, int scheme, int precision, double dt, double radius, int members,
+               mcv_handle **out);
+
+/* Upload the grid geometry computed by the caller's mesh setup
+ * (src/mesh_mod.F90:57-214, src/ghost_mod.f90:21-79): sqrtG, matrixG,
+ * matrixIG, matrixA, matrixIA, f over the padded range, and the ghost
+ * interpolation weights ghost%iref / ghost%coef as (nPVx, nPVHalo) arrays. */
+int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double *matrixG, const double *matrixIG,
+                     const double *matrixA, const double *matrixIA, const double *f, const int *ghost_iref,
+                     const double *ghost_coef);
+
+/* Upload member m's surface geopotential phi_s and its state: covariant u, v
+ * and phi over the full padded range, halo included (the first stage of the
+ * first step reads the caller's halo as src/time_scheme_mod.F90:27 does). */
+int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const double *u, const double *v, const double *phi);
+
+/* Advance every member by nsteps RK steps (the loop of src/MCV_SW.F90:57-77
+ * without history output).  Blocks until the steps are done. */
+int mcv_step(mcv_handle *h, int nsteps);
+
+/* Queue nsteps on the handle's stream and return without waiting. */
+int mcv_step_async(mcv_handle *h, int nsteps);
+/* Wait for queued work; returns MCV_ERR_NONFINITE if checking was on and a
+ * member went non-finite. */
+int mcv_sync(mcv_handle *h);
+
+/* Download member m's state over the padded range (any pointer may be NULL).
+ * phiG = phi * sqrtG as src/time_scheme_mod.F90:85 stores it. */
+int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double *phi, double *phiG);
+
+/* Total mass and energy of member m, with the quadrature of
+ * calc_total_mass / calc_total_energy (src/diag_mod.F90:10-67), summed on the
+ * device in FP64 with compensated (Neumaier) summation. */
+int mcv_mass_energy(mcv_handle *h, int m, double *mass, double *energy);
+
+/* Instrumentation (no counterpart in the reference, which only prints its
+ * total wall time, src/MCV_SW.F90:80-82).
+ * mcv_time_steps: advance nsteps and return their device time (CUDA events on
+ * the handle's stream around the replayed step graphs).
+ * mcv_profile_step: advance nsteps launching every kernel directly with events
+ * around each; returns the mean device time per launch of each stage kernel
+ * (stage_ms[0..3], unused stages 0) and of the halo kernel. */
+int mcv_time_steps(mcv_handle *h, int nsteps, double *ms);
+int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, double *halo_ms);
+
+/* Release the handle and its device memory. */
+int mcv_destroy(mcv_handle *h);
+
+/* Sizes of the grid: npx (padded points per direction), n (= nPVx), halo. */
+int mcv_grid_sizes(int order, int nc, int *npx, int *n, int *halo);
+
+/* Device bytes a handle with these arguments allocates (admission control). */
+long long mcv_footprint_bytes(int order, int nc, int scheme, int precision, int members);
+
+/* ---------------------------------------------------------------------
+ * Host-side init chain (the caller's side of the boundary; provided so C,
+ * C++ and Python callers without the Fortran setup can build inputs).
+ * ------------------------------------------------------------------- */
+
+/* Restates initMesh + initGhost (src/mesh_mod.F90:57-214,
+ * src/projection_mod.F90:8-322, src/ghost_mod.f90:21-79): fills every padded
+ * array; any output may be NULL. */
+int mcv_build_geometry(int order, int nc, double radius, double *lonP, double *latP, double *sqrtG, double *matrixG,
+                       double *matrixIG, double *matrixA, double *matrixIA, double *f, int *ghost_iref,
+                       double *ghost_coef);
+
+/* Williamson test cases 2, 5, 6 as initTestCase sets them
+ * (src/test_case_mod.F90:52-191): sphere winds, phi and phi_s on the padded
+ * points from lonP/latP. */
+int mcv_ic_williamson(int case_num, long long npts, const double *lonP, const double *latP, double radius,
+                      double *zonal, double *merid, double *phi, double *phi_s);
+
+/* Balanced solid-body zonal flow with its axis tilted by alpha (the case-5
+ * formulas of src/test_case_mod.F90:118-120 with no mountain). */
+int mcv_ic_tilted_zonal(long long npts, const double *lonP, const double *latP, double radius, double gh0, double u0,
+                        double alpha, double *zonal, double *merid, double *phi);
+
+/* phi += scale * sum_{l=1..lmax, m=-l..l} c[l*l + l + m] * Y_lm(lon, lat),
+ * with orthonormal real spherical harmonics (integral of Y^2 over the unit
+ * sphere = 1). */
+int mcv_ic_add_harmonics(long long npts, const double *lonP, const double *latP, int lmax, const double *coef,
+                         double scale, double *phi);
+
+/* Gaussian mountain hs = h0 * exp(-(d/efold)^2), d the great-circle distance
+ * (m) to (lon_c, lat_c): phi_s = g*hs, phi -= g*hs (test_case_mod.F90:117-128). */
+int mcv_ic_add_mountain(long long npts, const double *lonP, const double *latP, double radius, double lon_c,
+                        double lat_c, double h0, double efold, double *phi, double *phi_s);
+
+/* Adds one Rossby-Haurwitz wave of zonal wavenumber R (the case-6 formulas of
+ * src/test_case_mod.F90:133-191 with wave number R and angular velocity omg,
+ * without the constant gravity*h0) to zonal, merid and phi. */
+int mcv_ic_add_rossby_haurwitz(long long npts, const double *lonP, const double *latP, double radius, int R,
+                               double omg, double *zonal, double *merid, double *phi);
+
+/* Covariant winds from sphere winds, (u,v) = (G IA)(zonal, merid), as
+ * initTestCase does (src/test_case_mod.F90:32-39, projection_mod.F90:60-77). */
+int mcv_sphere_to_cov(long long npts, const double *matrixG, const double *matrixIA, const double *zonal,
+                      const double *merid, double *u, double *v);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCV_GPU_H */

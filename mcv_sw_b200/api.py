@@ -1,0 +1,270 @@
+"""ctypes binding of libmcv_gpu.so (include/mcv_gpu.h).
+
+Arrays use the reference's layout: a padded field is a C-contiguous numpy array
+of shape (6, npx, npx) -- identical in memory to Fortran's (i, j, panel) with
+i fastest -- and a 2x2 matrix field has shape (6, npx, npx, 2, 2) holding
+M(a, b) at [..., b-1, a-1] (Fortran's (2, 2, i, j, panel)).
+
+There is no CPU path: loading the library or creating a stepper raises
+``MCVError`` when the library is missing or no sm_100 GPU is present.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+RK3_TVD, RK4 = 3, 4
+FP64, MIXED = 0, 1
+SCHEMES = {"RK3_TVD": RK3_TVD, "RK4": RK4}
+PRECISIONS = {"fp64": FP64, "mixed": MIXED}
+
+_lib = None
+
+
+class MCVError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def lib_path():
+    return _build.LIB_PATH
+
+
+def lib():
+    """Load libmcv_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB_PATH
+    if not os.path.exists(path):
+        raise MCVError(-2, f"{path} is missing: run `python -m mcv_sw_b200.build` (there is no CPU fallback)")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    sig = {
+        "mcv_last_error": (ctypes.c_char_p, []),
+        "mcv_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, ctypes.POINTER(vp)]),
+        "mcv_set_geometry": (ctypes.c_int, [vp, _D, _D, _D, _D, _D, _D, _I, _D]),
+        "mcv_set_member": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
+        "mcv_step": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mcv_step_async": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mcv_sync": (ctypes.c_int, [vp]),
+        "mcv_get_state": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
+        "mcv_mass_energy": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
+        "mcv_destroy": (ctypes.c_int, [vp]),
+        "mcv_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _D]),
+        "mcv_profile_step": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
+        "mcv_grid_sizes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _I, _I, _I]),
+        "mcv_footprint_bytes": (ctypes.c_longlong, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int]),
+        "mcv_build_geometry": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D, _D, _D, _D, _D,
+                                              _D, _D, _I, _D]),
+        "mcv_ic_williamson": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, _D, _D, ctypes.c_double, _D, _D, _D,
+                                             _D]),
+        "mcv_ic_tilted_zonal": (ctypes.c_int, [ctypes.c_longlong, _D, _D, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, _D, _D, _D]),
+        "mcv_ic_add_harmonics": (ctypes.c_int, [ctypes.c_longlong, _D, _D, ctypes.c_int, _D, ctypes.c_double, _D]),
+        "mcv_ic_add_mountain": (ctypes.c_int, [ctypes.c_longlong, _D, _D, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_double, _D, _D]),
+        "mcv_ic_add_rossby_haurwitz": (ctypes.c_int, [ctypes.c_longlong, _D, _D, ctypes.c_double, ctypes.c_int,
+                                                      ctypes.c_double, _D, _D, _D]),
+        "mcv_sphere_to_cov": (ctypes.c_int, [ctypes.c_longlong, _D, _D, _D, _D, _D, _D]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise MCVError(rc, lib().mcv_last_error().decode())
+    return rc
+
+
+def _dp(a):
+    if a is None:
+        return None
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_D)
+
+
+def _ip(a):
+    if a.dtype != np.int32 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("expected a C-contiguous int32 array")
+    return a.ctypes.data_as(_I)
+
+
+def grid_sizes(order, nc):
+    npx, n, h = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().mcv_grid_sizes(int(order), int(nc), ctypes.byref(npx), ctypes.byref(n), ctypes.byref(h)))
+    return npx.value, n.value, h.value
+
+
+def footprint_bytes(order, nc, scheme="RK3_TVD", precision="fp64", members=1):
+    return int(lib().mcv_footprint_bytes(int(order), int(nc), SCHEMES[scheme], PRECISIONS[precision], int(members)))
+
+
+class Geometry:
+    """initMesh + initGhost on the host (mcv_build_geometry)."""
+
+    def __init__(self, order, nc, radius=6371220.0):
+        self.order, self.nc, self.radius = int(order), int(nc), float(radius)
+        self.npx, self.n, self.H = grid_sizes(order, nc)
+        shp = (6, self.npx, self.npx)
+        self.lonP, self.latP, self.sqrtG, self.f = (np.empty(shp) for _ in range(4))
+        self.matrixG, self.matrixIG, self.matrixA, self.matrixIA = (np.empty(shp + (2, 2)) for _ in range(4))
+        self.ghost_iref = np.empty((self.H, self.n), dtype=np.int32)
+        self.ghost_coef = np.empty((self.H, self.n))
+        _check(lib().mcv_build_geometry(self.order, self.nc, self.radius, _dp(self.lonP), _dp(self.latP),
+                                        _dp(self.sqrtG), _dp(self.matrixG), _dp(self.matrixIG), _dp(self.matrixA),
+                                        _dp(self.matrixIA), _dp(self.f), _ip(self.ghost_iref), _dp(self.ghost_coef)))
+        self.dx = (90.0 / self.nc) * (2.0 * np.arcsin(1.0) / 180.0)
+
+    @property
+    def shape(self):
+        return (6, self.npx, self.npx)
+
+    @property
+    def npts(self):
+        return 6 * self.npx * self.npx
+
+    def interior(self, a):
+        H, n = self.H, self.n
+        return a[:, H:H + n, H:H + n]
+
+    def pv_weights(self):
+        """Quadrature weight of every padded point: weightsOnPV summed over the
+        cells that share the point (mesh_mod.F90:183-203), zero in the halo."""
+        D = self.order
+        w1 = np.array([1.0, 4.0, 1.0]) / 6.0 if D == 3 else np.array([1.0, 3.0, 3.0, 1.0]) / 8.0
+        line = np.zeros(self.npx)
+        for c in range(self.nc):
+            line[self.H + c * (D - 1): self.H + c * (D - 1) + D] += w1
+        return np.broadcast_to(np.outer(line, line), self.shape)
+
+
+# ---------------------------------------------------------------- initial conditions
+def williamson(geom, case_num):
+    shp = geom.shape
+    zw, mw, phi, phis = (np.empty(shp) for _ in range(4))
+    _check(lib().mcv_ic_williamson(int(case_num), geom.npts, _dp(geom.lonP), _dp(geom.latP), geom.radius, _dp(zw),
+                                   _dp(mw), _dp(phi), _dp(phis)))
+    return zw, mw, phi, phis
+
+
+def tilted_zonal(geom, gh0, u0, alpha):
+    shp = geom.shape
+    zw, mw, phi = (np.empty(shp) for _ in range(3))
+    _check(lib().mcv_ic_tilted_zonal(geom.npts, _dp(geom.lonP), _dp(geom.latP), geom.radius, float(gh0), float(u0),
+                                     float(alpha), _dp(zw), _dp(mw), _dp(phi)))
+    return zw, mw, phi
+
+
+def add_harmonics(geom, phi, coef, scale=1.0):
+    coef = np.ascontiguousarray(coef, dtype=np.float64)
+    lmax = int(round(np.sqrt(coef.size))) - 1
+    assert (lmax + 1) ** 2 == coef.size
+    _check(lib().mcv_ic_add_harmonics(geom.npts, _dp(geom.lonP), _dp(geom.latP), lmax, _dp(coef), float(scale),
+                                      _dp(phi)))
+
+
+def add_mountain(geom, phi, phis, lon_c, lat_c, h0=2000.0, efold=1.0e6):
+    _check(lib().mcv_ic_add_mountain(geom.npts, _dp(geom.lonP), _dp(geom.latP), geom.radius, float(lon_c),
+                                     float(lat_c), float(h0), float(efold), _dp(phi), _dp(phis)))
+
+
+def add_rossby_haurwitz(geom, zw, mw, phi, wavenumber, omg):
+    _check(lib().mcv_ic_add_rossby_haurwitz(geom.npts, _dp(geom.lonP), _dp(geom.latP), geom.radius, int(wavenumber),
+                                            float(omg), _dp(zw), _dp(mw), _dp(phi)))
+
+
+def sphere_to_cov(geom, zw, mw):
+    u, v = np.empty(geom.shape), np.empty(geom.shape)
+    _check(lib().mcv_sphere_to_cov(geom.npts, _dp(geom.matrixG), _dp(geom.matrixIA), _dp(zw), _dp(mw), _dp(u),
+                                   _dp(v)))
+    return u, v
+
+
+# ---------------------------------------------------------------- stepping
+class Stepper:
+    """One device-resident ensemble of `members` states on one grid."""
+
+    def __init__(self, order, nc, dt, scheme="RK3_TVD", members=1, precision="fp64", radius=6371220.0):
+        self.order, self.nc, self.dt, self.scheme = int(order), int(nc), float(dt), scheme
+        self.members, self.precision = int(members), precision
+        self.npx, self.n, self.H = grid_sizes(order, nc)
+        h = ctypes.c_void_p()
+        _check(lib().mcv_create(self.order, self.nc, SCHEMES[scheme], PRECISIONS[precision], self.dt, float(radius),
+                                self.members, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mcv_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_geometry(self, geom):
+        _check(lib().mcv_set_geometry(self.h, _dp(geom.sqrtG), _dp(geom.matrixG), _dp(geom.matrixIG),
+                                      _dp(geom.matrixA), _dp(geom.matrixIA), _dp(geom.f), _ip(geom.ghost_iref),
+                                      _dp(geom.ghost_coef)))
+
+    def set_member(self, m, phi_s, u, v, phi):
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (phi_s, u, v, phi)]
+        _check(lib().mcv_set_member(self.h, int(m), *[_dp(x) for x in arrs]))
+
+    def step(self, nsteps=1):
+        _check(lib().mcv_step(self.h, int(nsteps)))
+
+    def step_async(self, nsteps=1):
+        _check(lib().mcv_step_async(self.h, int(nsteps)))
+
+    def sync(self):
+        _check(lib().mcv_sync(self.h))
+
+    def get_state(self, m=0, out=None):
+        shp = (6, self.npx, self.npx)
+        out = out or {k: np.empty(shp) for k in ("u", "v", "phi", "phiG")}
+        _check(lib().mcv_get_state(self.h, int(m), _dp(out.get("u")), _dp(out.get("v")), _dp(out.get("phi")),
+                                   _dp(out.get("phiG"))))
+        return out
+
+    def time_steps(self, nsteps):
+        """Advance nsteps; device milliseconds (CUDA events on the library stream)."""
+        ms = ctypes.c_double()
+        _check(lib().mcv_time_steps(self.h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def profile_step(self, nsteps=1):
+        """Advance nsteps with per-launch events: (mean ms per stage kernel, mean ms per halo kernel)."""
+        st = (ctypes.c_double * 4)()
+        ha = ctypes.c_double()
+        _check(lib().mcv_profile_step(self.h, int(nsteps), st, ctypes.byref(ha)))
+        nst = 3 if self.scheme == "RK3_TVD" else 4
+        return list(st)[:nst], ha.value
+
+    def mass_energy(self, m=0):
+        ms, en = ctypes.c_double(), ctypes.c_double()
+        _check(lib().mcv_mass_energy(self.h, int(m), ctypes.byref(ms), ctypes.byref(en)))
+        return ms.value, en.value

@@ -1,0 +1,170 @@
+"""Seeded synthetic initial states for the benchmark workloads.
+
+Every state is evaluated at each padded point's own lon/lat, halo included, as
+initTestCase does (src/test_case_mod.F90:13-49), then projected to covariant
+winds with (G IA) (test_case_mod.F90:32-39).  The base flow is the balanced
+solid-body zonal flow with a tilted axis (the case-5 formulas,
+test_case_mod.F90:118-120, without the mountain); perturbations are seeded real
+spherical harmonics rescaled to a stated area-weighted RMS height, Gaussian
+mountains (phi_s = g hs, phi -= g hs as in test_case_mod.F90:117-128) and
+Rossby-Haurwitz waves (test_case_mod.F90:133-191 with other wave numbers).
+
+Workload sizes follow the project's five configurations:
+  small     MCV3, Nc=32,  RK4,  tilted zonal + harmonics deg 1-8 (RMS 10 m), 1 day
+  large     MCV4, Nc=256, RK3,  + harmonics deg <=32 (RMS 20 m) + mountain, 5 days
+  ensemble  MCV3, Nc=128, RK4,  64 members, harmonics deg <=16 RMS U(5,30) m,
+            alpha U[0, pi/2], u0 U[20, 40] m/s, 2 days
+  serving   MCV3/MCV4, Nc in {48, 96, 192, 384}, 6-120 h, half with mountains
+  stress    MCV4, Nc=1024, RK4, zonal waves R=4..12 (50-200 m), 200 steps
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import api
+
+GRAVITY = 9.80616
+EARTH_RADIUS = 6.371e6
+GH0 = 2.94e4
+
+
+@dataclass
+class InitialState:
+    order: int
+    nc: int
+    scheme: str
+    dt: float
+    nsteps: int
+    phi_s: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    phi: np.ndarray
+    zonal: np.ndarray = None
+    merid: np.ndarray = None
+    meta: dict = field(default_factory=dict)
+
+
+def area_rms(geom, h):
+    """Area-weighted RMS over the sphere with the PV quadrature weights."""
+    w = geom.pv_weights() * geom.sqrtG
+    return float(np.sqrt(np.sum(w * h * h) / np.sum(w)))
+
+
+def harmonic_height(geom, rng, lmin, lmax, rms):
+    """Random real spherical harmonics of degree lmin..lmax with Gaussian
+    coefficients, rescaled to the area-weighted RMS `rms` (metres)."""
+    coef = rng.standard_normal((lmax + 1) ** 2)
+    coef[: lmin * lmin] = 0.0
+    h = np.zeros(geom.shape)
+    api.add_harmonics(geom, h, coef, 1.0)
+    return h * (rms / area_rms(geom, h))
+
+
+def cfl_dt(geom, u, v, phi, cfl=0.5):
+    """dt = cfl * (dx/(D-1)) / max over interior PVs of |c^i| + sqrt(G^ii phi)."""
+    IG = geom.matrixIG
+    cu = IG[..., 0, 0] * u + IG[..., 1, 0] * v
+    cv = IG[..., 0, 1] * u + IG[..., 1, 1] * v
+    sx = np.abs(cu) + np.sqrt(IG[..., 0, 0] * phi)
+    sy = np.abs(cv) + np.sqrt(IG[..., 1, 1] * phi)
+    smax = max(float(geom.interior(sx).max()), float(geom.interior(sy).max()))
+    return cfl * (geom.dx / (geom.order - 1)) / smax
+
+
+def fit_steps(dt_cfl, seconds):
+    """Largest dt <= dt_cfl that divides the run length exactly."""
+    nsteps = int(math.ceil(seconds / dt_cfl))
+    return seconds / nsteps, nsteps
+
+
+def finish(geom, zw, mw, phi, phis, scheme, seconds=None, nsteps=None, cfl=0.5, meta=None):
+    u, v = api.sphere_to_cov(geom, zw, mw)
+    dt_cfl = cfl_dt(geom, u, v, phi, cfl)
+    if seconds is not None:
+        dt, ns = fit_steps(dt_cfl, seconds)
+    else:
+        dt, ns = dt_cfl, int(nsteps)
+    return InitialState(geom.order, geom.nc, scheme, dt, ns, phis, u, v, phi, zw, mw, meta or {})
+
+
+def balanced_flow(geom, rng, u0=38.6, alpha=0.05, lmax=8, rms=10.0, mountain=False, lmin=1):
+    zw, mw, phi = api.tilted_zonal(geom, GH0, u0, alpha)
+    phis = np.zeros(geom.shape)
+    if lmax:
+        phi += GRAVITY * harmonic_height(geom, rng, lmin, lmax, rms)
+    meta = {"u0": u0, "alpha": alpha, "lmax": lmax, "rms_m": rms}
+    if mountain:
+        lon_c = rng.uniform(0.0, 2.0 * np.pi)
+        lat_c = np.arcsin(rng.uniform(-0.8, 0.8))
+        api.add_mountain(geom, phi, phis, lon_c, lat_c, 2000.0, 1.0e6)
+        meta.update(mountain_lon=lon_c, mountain_lat=lat_c)
+    return zw, mw, phi, phis, meta
+
+
+def small(seed=1, nc=32, order=3, scheme="RK4", days=1.0, geom=None):
+    geom = geom or api.Geometry(order, nc, EARTH_RADIUS)
+    rng = np.random.default_rng(seed)
+    zw, mw, phi, phis, meta = balanced_flow(geom, rng, 38.6, 0.05, 8, 10.0)
+    return finish(geom, zw, mw, phi, phis, scheme, seconds=days * 86400.0, meta=meta), geom
+
+
+def large(seed=2, nc=256, order=4, scheme="RK3_TVD", days=5.0, geom=None):
+    geom = geom or api.Geometry(order, nc, EARTH_RADIUS)
+    rng = np.random.default_rng(seed)
+    zw, mw, phi, phis, meta = balanced_flow(geom, rng, 38.6, 0.05, 32, 20.0, mountain=True)
+    return finish(geom, zw, mw, phi, phis, scheme, seconds=days * 86400.0, meta=meta), geom
+
+
+def ensemble_member(geom, seed, scheme="RK4", days=2.0):
+    rng = np.random.default_rng(seed)
+    alpha = rng.uniform(0.0, np.pi / 2)
+    u0 = rng.uniform(20.0, 40.0)
+    rms = rng.uniform(5.0, 30.0)
+    zw, mw, phi, phis, meta = balanced_flow(geom, rng, u0, alpha, 16, rms)
+    return finish(geom, zw, mw, phi, phis, scheme, seconds=days * 86400.0, meta=meta)
+
+
+def stress(seed=5, nc=1024, order=4, scheme="RK4", nsteps=200, geom=None):
+    geom = geom or api.Geometry(order, nc, EARTH_RADIUS)
+    rng = np.random.default_rng(seed)
+    zw, mw, phi = api.tilted_zonal(geom, GH0, 38.6, 0.05)
+    phis = np.zeros(geom.shape)
+    waves = []
+    for R in range(4, 13):
+        amp = rng.uniform(50.0, 200.0)
+        # angular velocity giving a height amplitude ~amp for wave number R
+        c = max(abs(np.cos(t) ** R * ((R * R + 2 * R + 2) - (R + 1) ** 2 * np.cos(t) ** 2))
+                for t in np.linspace(-1.5, 1.5, 301))
+        omg = amp * GRAVITY * (R + 1) * (R + 2) / (2.0 * 7.292e-5 * geom.radius ** 2 * c)
+        api.add_rossby_haurwitz(geom, zw, mw, phi, R, omg)
+        waves.append((R, amp))
+    # the helper adds each wave's zonal-mean geopotential too; keep the mean depth
+    phi += GH0 - area_mean(geom, phi)
+    return finish(geom, zw, mw, phi, phis, scheme, nsteps=nsteps, meta={"waves": waves}), geom
+
+
+def area_mean(geom, a):
+    w = geom.pv_weights() * geom.sqrtG
+    return float(np.sum(w * a) / np.sum(w))
+
+
+def serving_requests(seed=4, rate=20.0, count=64):
+    """Poisson arrivals: (t_arrive, order, nc, hours, mountain, seed)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    for k in range(count):
+        t += rng.exponential(1.0 / rate)
+        order = 3 if rng.uniform() < 0.5 else 4
+        nc = int(rng.choice([48, 96, 192, 384], p=[0.4, 0.3, 0.2, 0.1]))
+        hours = float(rng.uniform(6.0, 120.0))
+        reqs.append(dict(t=t, order=order, nc=nc, hours=hours, mountain=bool(rng.uniform() < 0.5),
+                         seed=int(rng.integers(1 << 31)), id=k))
+    return reqs
+
+
+def serving_state(geom, req, scheme="RK3_TVD"):
+    rng = np.random.default_rng(req["seed"])
+    zw, mw, phi, phis, meta = balanced_flow(geom, rng, 38.6, 0.05, 8, 10.0, mountain=req["mountain"])
+    return finish(geom, zw, mw, phi, phis, scheme, seconds=req["hours"] * 3600.0, meta=meta)
