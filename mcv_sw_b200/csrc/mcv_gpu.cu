@@ -85,11 +85,11 @@ template <int D>
 struct TileShape;
 template <>
 struct TileShape<3> {
-  static constexpr int CX = 12, CY = 12, NT = 256;
+  static constexpr int CX = 12, CY = 12, NT = 320;
 };
 template <>
 struct TileShape<4> {
-  static constexpr int CX = 8, CY = 8, NT = 256;
+  static constexpr int CX = 8, CY = 8, NT = 320;
 };
 
 }  // namespace mcv
@@ -230,7 +230,7 @@ void launch_halo(mcv_handle *h, double *const st[3]) {
   a.dx2 = h->dx2;
   a.dx3 = h->dx3;
   a.members = h->members;
-  const long long threads = 24LL * h->g.n * h->members;
+  const long long threads = 24LL * (h->H + 1) * h->g.n * h->members;
   const int block = 128;
   halo_kernel<D><<<(unsigned)((threads + block - 1) / block), block, 0, h->stream>>>(h->g, a);
 }
@@ -341,6 +341,9 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   grid_desc(order, nc, h->g, h->H, h->npx);
   const double pi = 2.0 * std::asin(1.0);
   h->g.dx = (90. / nc) * (pi / 180.);
+  h->g.inv_dx = 1. / h->g.dx;
+  h->g.inv_2dx = 1. / (2. * h->g.dx);
+  h->g.inv_dx2 = 1. / (h->g.dx * h->g.dx);
   h->dx2 = h->g.dx * h->g.dx;
   h->dx3 = std::pow(h->g.dx, 3.);
   int CX = order == 3 ? TileShape<3>::CX : TileShape<4>::CX, CY = order == 3 ? TileShape<3>::CY : TileShape<4>::CY;

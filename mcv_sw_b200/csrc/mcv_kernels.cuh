@@ -40,6 +40,7 @@ struct GridDesc {
   long long plane;    // np * P
   long long mstride;  // 6 * plane
   double dx;          // cell width in radians
+  double inv_dx, inv_2dx, inv_dx2;  // 1/dx, 1/(2 dx), 1/dx**2
 };
 
 struct StageArgs {
@@ -82,17 +83,20 @@ __constant__ EdgeLink c_links[6][4];
 __constant__ VertexRef c_vertex[6][4];  // indexed by (panel, corner) of the owner
 
 // ---------------------------------------------------------------------------
-// One-dimensional MCV building blocks (src/spatial_operators_mod.F90:136-246)
+// One-dimensional MCV building blocks (src/spatial_operators_mod.F90:136-246).
+// Divisions by the cell width are multiplications by precomputed reciprocals
+// (GridDesc::inv_dx, inv_2dx), one rounding away from the reference's quotient.
 // ---------------------------------------------------------------------------
 template <int D>
-__device__ __forceinline__ double polyfit_left(const double *pv, double dh) {
-  if constexpr (D == 3) return -(pv[2] - 4. * pv[1] + 3. * pv[0]) / dh;
-  else return (-(11. * pv[0]) + 18. * pv[1] - 9. * pv[2] + 2. * pv[3]) / (2. * dh);
+__device__ __forceinline__ double polyfit_left(const double *pv, double inv) {
+  // inv = 1/dh (MCV3) or 1/(2 dh) (MCV4)
+  if constexpr (D == 3) return -(pv[2] - 4. * pv[1] + 3. * pv[0]) * inv;
+  else return (-(11. * pv[0]) + 18. * pv[1] - 9. * pv[2] + 2. * pv[3]) * inv;
 }
 template <int D>
-__device__ __forceinline__ double polyfit_right(const double *pv, double dh) {
-  if constexpr (D == 3) return (pv[0] - 4. * pv[1] + 3. * pv[2]) / dh;
-  else return (11. * pv[3] - 18. * pv[2] + 9. * pv[1] - 2. * pv[0]) / (2. * dh);
+__device__ __forceinline__ double polyfit_right(const double *pv, double inv) {
+  if constexpr (D == 3) return (pv[0] - 4. * pv[1] + 3. * pv[2]) * inv;
+  else return (11. * pv[3] - 18. * pv[2] + 9. * pv[1] - 2. * pv[0]) * inv;
 }
 __device__ __forceinline__ double riemann(double fL, double fR, double qL, double qR, double lam) {
   return 0.5 * ((fL + fR) - lam * (qR - qL));
@@ -102,40 +106,32 @@ __device__ __forceinline__ double riemann(double fL, double fR, double qL, doubl
 // (3D-2 values with stride S): calc_tendP, src/spatial_operators_mod.F90:136-202.
 template <int D, int S>
 __device__ __forceinline__ void cell_derivs(double out[D], const double *f, const double *q, double lamL,
-                                            double lamR, double dx) {
-  double c1[D], c2[D], c3[D];
+                                            double lamR, const GridDesc &g) {
+  const double ip = (D == 3) ? g.inv_dx : g.inv_2dx;
+  double c1[D], c2[D], c3[D], d1[D], d2[D], d3[D];
 #pragma unroll
   for (int m = 0; m < D; ++m) {
     c1[m] = f[m * S];
     c2[m] = f[(D - 1 + m) * S];
     c3[m] = f[(2 * D - 2 + m) * S];
+    d1[m] = q[m * S];
+    d2[m] = q[(D - 1 + m) * S];
+    d3[m] = q[(2 * D - 2 + m) * S];
   }
-  const double fxL1 = polyfit_right<D>(c1, dx), fxL2 = polyfit_right<D>(c2, dx);
-  const double fxR1 = polyfit_left<D>(c2, dx), fxR2 = polyfit_left<D>(c3, dx);
-  double qxL1, qxL2, qxR1, qxR2;
-  if (f == q) {
-    qxL1 = fxL1; qxL2 = fxL2; qxR1 = fxR1; qxR2 = fxR2;
-  } else {
-    double d1[D], d2[D], d3[D];
-#pragma unroll
-    for (int m = 0; m < D; ++m) {
-      d1[m] = q[m * S];
-      d2[m] = q[(D - 1 + m) * S];
-      d3[m] = q[(2 * D - 2 + m) * S];
-    }
-    qxL1 = polyfit_right<D>(d1, dx); qxL2 = polyfit_right<D>(d2, dx);
-    qxR1 = polyfit_left<D>(d2, dx); qxR2 = polyfit_left<D>(d3, dx);
-  }
+  const double fxL1 = polyfit_right<D>(c1, ip), fxL2 = polyfit_right<D>(c2, ip);
+  const double fxR1 = polyfit_left<D>(c2, ip), fxR2 = polyfit_left<D>(c3, ip);
+  const double qxL1 = polyfit_right<D>(d1, ip), qxL2 = polyfit_right<D>(d2, ip);
+  const double qxR1 = polyfit_left<D>(d2, ip), qxR2 = polyfit_left<D>(d3, ip);
   out[0] = riemann(fxL1, fxR1, qxL1, qxR1, lamL);
   out[D - 1] = riemann(fxL2, fxR2, qxL2, qxR2, lamR);
   if constexpr (D == 3) {
-    const double fxVIA = (c2[2] - c2[0]) / dx;
+    const double fxVIA = (c2[2] - c2[0]) * g.inv_dx;
     out[1] = 1.5 * fxVIA - 0.25 * (out[0] + out[2]);
   } else {
-    const double fxVIA = (c2[3] - c2[0]) / dx;
-    const double fxxc = 4.5 * (c2[0] - c2[1] - c2[2] + c2[3]) / (dx * dx);
-    out[1] = 4. / 3. * fxVIA - (4. * out[0] + 5. * out[3]) / 27. - 4. / 27. * dx * fxxc;
-    out[2] = 4. / 3. * fxVIA - (5. * out[0] + 4. * out[3]) / 27. + 4. / 27. * dx * fxxc;
+    const double fxVIA = (c2[3] - c2[0]) * g.inv_dx;
+    const double fxxc = 4.5 * (c2[0] - c2[1] - c2[2] + c2[3]) * g.inv_dx2;
+    out[1] = 4. / 3. * fxVIA - (4. * out[0] + 5. * out[3]) / 27. - 4. / 27. * g.dx * fxxc;
+    out[2] = 4. / 3. * fxVIA - (5. * out[0] + 4. * out[3]) / 27. + 4. / 27. * g.dx * fxxc;
   }
 }
 
@@ -149,23 +145,24 @@ struct Tile {
   static constexpr int TY = CY * (D - 1) + 1;
   static constexpr int LX = TX + 2 * H;        // loaded row length (odd: no bank conflicts on column walks)
   static constexpr int LY = TY + 2 * H;
-  static constexpr int W = 3 * D - 2;          // 3-cell window
   static constexpr int A = LX * LY;
+  static constexpr int I = TX * TY;
   // shared-memory carve (doubles)
   static constexpr int U = 0, V = A, E = 2 * A, PG = 3 * A, PGU = 4 * A, PGV = 5 * A, CU = 6 * A, CV = 7 * A,
                        SG = 8 * A;
-  static constexpr int LAMX = 9 * A;              // [TY][CX+1]
+  static constexpr int LAMX = 9 * A;                 // [TY][CX+1]
   static constexpr int SGNX = LAMX + TY * (CX + 1);
   static constexpr int LAMY = SGNX + TY * (CX + 1);  // [TX][CY+1]
   static constexpr int SGNY = LAMY + TX * (CY + 1);
-  static constexpr int XR = SGNY + TX * (CY + 1);     // x-sweep results [3][TY][TX]
-  static constexpr int TOTAL = XR + 3 * TY * TX;
+  static constexpr int XR = SGNY + TX * (CY + 1);    // x-sweep results [3][TY][TX]
+  static constexpr int YR = XR + 3 * I;              // y-sweep results [3][TY][TX]
+  static constexpr int TOTAL = YR + 3 * I;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(double);
   static_assert(LX % 2 == 1, "odd shared row length");
 };
 
 template <int D, int CX, int CY, int NT, int KIND>
-__global__ void __launch_bounds__(NT, 2) stage_kernel(const GridDesc g, const StageArgs a) {
+__global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const StageArgs a) {
   using T = Tile<D, CX, CY>;
   constexpr int H = T::H, LX = T::LX;
   extern __shared__ double sm[];
@@ -180,150 +177,184 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const GridDesc g, const St
 
   // ---- phase 0: load the tile and its halo cross, pointwise quantities ----
   // (spatial_operators_mod.F90:58-61, eigenvalues :248-280, upwind signs :83-85)
-  for (int idx = threadIdx.x; idx < T::A; idx += NT) {
-    const int ly = idx / LX, lx = idx - ly * LX;
-    if (lx >= lxe || ly >= lye) continue;
-    const bool xh = (lx < H) || (lx >= lxe - H);
-    const bool yh = (ly < H) || (ly >= lye - H);
-    if (xh && yh) continue;  // tile corner: never read by either sweep
-    const long long go = (long long)(Y0 + ly) * g.P + (X0 + lx);
-    const double u = a.us[mbase + go], v = a.vs[mbase + go], phi = a.ps[mbase + go];
-    const double sg = __ldg(a.sqrtG + pbase + go);
-    const double g11 = __ldg(a.ig11 + pbase + go), g12 = __ldg(a.ig12 + pbase + go), g22 = __ldg(a.ig22 + pbase + go);
-    const double phs = __ldg(a.phis + mbase + go);
-    const double cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
-    const double cv = g12 * u + g22 * v;
-    const double pg = phi * sg;
-    const double K = 0.5 * (cu * u + cv * v);
-    sm[T::U + idx] = u;
-    sm[T::V + idx] = v;
-    sm[T::CU + idx] = cu;
-    sm[T::CV + idx] = cv;
-    sm[T::PG + idx] = pg;
-    sm[T::PGU + idx] = pg * cu;
-    sm[T::PGV + idx] = pg * cv;
-    sm[T::E + idx] = phi + phs + K;
-    sm[T::SG + idx] = sg;
-    if (!xh && !yh) {
-      const int ix = lx - H, iy = ly - H;
-      // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
-      if (ix % (D - 1) == 0) {
-        sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
-        sm[T::SGNX + iy * (CX + 1) + ix / (D - 1)] = (cu < 0.) ? -1. : 1.;
+  {
+    constexpr int PPT = (T::A + NT - 1) / NT;
+    double ru[PPT], rv[PPT], rp[PPT], rs[PPT], r11[PPT], r12[PPT], r22[PPT], rh[PPT];
+    bool ok[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const int idx = threadIdx.x + k * NT;
+      const int ly = idx / LX, lx = idx - ly * LX;
+      const bool xh = (lx < H) || (lx >= lxe - H);
+      const bool yh = (ly < H) || (ly >= lye - H);
+      ok[k] = idx < T::A && lx < lxe && ly < lye && !(xh && yh);  // tile corners are never read
+      if (ok[k]) {
+        const long long go = (long long)(Y0 + ly) * g.P + (X0 + lx);
+        ru[k] = __ldg(a.us + mbase + go);
+        rv[k] = __ldg(a.vs + mbase + go);
+        rp[k] = __ldg(a.ps + mbase + go);
+        rh[k] = __ldg(a.phis + mbase + go);
+        rs[k] = __ldg(a.sqrtG + pbase + go);
+        r11[k] = __ldg(a.ig11 + pbase + go);
+        r12[k] = __ldg(a.ig12 + pbase + go);
+        r22[k] = __ldg(a.ig22 + pbase + go);
       }
-      if (iy % (D - 1) == 0) {
-        sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
-        sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < 0.) ? -1. : 1.;
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      if (!ok[k]) continue;
+      const int idx = threadIdx.x + k * NT;
+      const int ly = idx / LX, lx = idx - ly * LX;
+      const double u = ru[k], v = rv[k], phi = rp[k], sg = rs[k], g11 = r11[k], g12 = r12[k], g22 = r22[k];
+      const double cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
+      const double cv = g12 * u + g22 * v;
+      const double pg = phi * sg;
+      const double K = 0.5 * (cu * u + cv * v);
+      sm[T::U + idx] = u;
+      sm[T::V + idx] = v;
+      sm[T::CU + idx] = cu;
+      sm[T::CV + idx] = cv;
+      sm[T::PG + idx] = pg;
+      sm[T::PGU + idx] = pg * cu;
+      sm[T::PGV + idx] = pg * cv;
+      sm[T::E + idx] = phi + rh[k] + K;
+      sm[T::SG + idx] = sg;
+      const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
+      if (!xh && !yh) {
+        const int ix = lx - H, iy = ly - H;
+        // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
+        if (ix % (D - 1) == 0) {
+          sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
+          sm[T::SGNX + iy * (CX + 1) + ix / (D - 1)] = (cu < 0.) ? -1. : 1.;
+        }
+        if (iy % (D - 1) == 0) {
+          sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
+          sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < 0.) ? -1. : 1.;
+        }
       }
     }
   }
   __syncthreads();
 
   const int txe = ncx * (D - 1) + 1, tye = ncy * (D - 1) + 1;
-  const double dx = g.dx;
 
-  // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), one (row, cell) per item ----
-  for (int it = threadIdx.x; it < T::TY * CX; it += NT) {
-    const int r = it % T::TY, c = it / T::TY;
+  // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), item = (row, cell, quantity) ----
+  // quantity 0: flux_x = d(E)/dx, Riemann on u; 1: div_x = d(phiG cU)/dx, Riemann
+  // on phiG; 2: dvdx, upwinded by sign(cU)
+  for (int it = threadIdx.x; it < T::TY * CX * 3; it += NT) {
+    const int r = it % T::TY, rest = it / T::TY;
+    const int c = rest % CX, k = rest / CX;
     if (r >= tye || c >= ncx) continue;
     const int w0 = (r + H) * LX + c * (D - 1);
-    const double lL = sm[T::LAMX + r * (CX + 1) + c], lR = sm[T::LAMX + r * (CX + 1) + c + 1];
-    const double sL = sm[T::SGNX + r * (CX + 1) + c], sR = sm[T::SGNX + r * (CX + 1) + c + 1];
+    const int fo = (k == 0) ? T::E : (k == 1) ? T::PGU : T::V;
+    const int qo = (k == 0) ? T::U : (k == 1) ? T::PG : T::V;
+    const int lo = (k == 2) ? T::SGNX : T::LAMX;
     double d[D];
+    cell_derivs<D, 1>(d, sm + fo + w0, sm + qo + w0, sm[lo + r * (CX + 1) + c], sm[lo + r * (CX + 1) + c + 1], g);
+    double *xr = sm + T::XR + k * T::I + r * T::TX + c * (D - 1);
     const int mmax = (c == ncx - 1) ? D : D - 1;
-    double *xr = sm + T::XR + r * T::TX + c * (D - 1);
-    cell_derivs<D, 1>(d, sm + T::E + w0, sm + T::U + w0, lL, lR, dx);  // flux_x
 #pragma unroll
     for (int m = 0; m < D; ++m)
       if (m < mmax) xr[m] = d[m];
-    cell_derivs<D, 1>(d, sm + T::PGU + w0, sm + T::PG + w0, lL, lR, dx);  // div_x
+  }
+
+  // ---- phase Y: y-sweep (:95-125), item = (column, cell, quantity) ----
+  for (int it = threadIdx.x; it < T::TX * CY * 3; it += NT) {
+    const int q = it % T::TX, rest = it / T::TX;
+    const int c = rest % CY, k = rest / CY;
+    if (q >= txe || c >= ncy) continue;
+    const int w0 = (c * (D - 1)) * LX + (q + H);
+    const int fo = (k == 0) ? T::E : (k == 1) ? T::PGV : T::U;
+    const int qo = (k == 0) ? T::V : (k == 1) ? T::PG : T::U;
+    const int lo = (k == 2) ? T::SGNY : T::LAMY;
+    double d[D];
+    cell_derivs<D, LX>(d, sm + fo + w0, sm + qo + w0, sm[lo + q * (CY + 1) + c], sm[lo + q * (CY + 1) + c + 1], g);
+    double *yr = sm + T::YR + k * T::I + (c * (D - 1)) * T::TX + q;
+    const int mmax = (c == ncy - 1) ? D : D - 1;
 #pragma unroll
     for (int m = 0; m < D; ++m)
-      if (m < mmax) xr[T::TY * T::TX + m] = d[m];
-    cell_derivs<D, 1>(d, sm + T::V + w0, sm + T::V + w0, sL, sR, dx);  // dvdx
-#pragma unroll
-    for (int m = 0; m < D; ++m)
-      if (m < mmax) xr[2 * T::TY * T::TX + m] = d[m];
+      if (m < mmax) yr[m * T::TX] = d[m];
   }
   __syncthreads();
 
-  // ---- phase Y: y-sweep (:95-125), tendency assembly (:127-131), RK update ----
+  // ---- phase A: tendency assembly (:127-131), RK stage update, store ----
   const bool last_x = (c0x + ncx == g.Nc), last_y = (c0y + ncy == g.Nc);
-  for (int it = threadIdx.x; it < T::TX * CY; it += NT) {
-    const int q = it % T::TX, c = it / T::TX;
-    if (q >= txe || c >= ncy) continue;
-    if (q == txe - 1 && !last_x) continue;  // column owned by the next tile
-    const int w0 = (c * (D - 1)) * LX + (q + H);
-    const double lL = sm[T::LAMY + q * (CY + 1) + c], lR = sm[T::LAMY + q * (CY + 1) + c + 1];
-    const double sL = sm[T::SGNY + q * (CY + 1) + c], sR = sm[T::SGNY + q * (CY + 1) + c + 1];
-    double fy[D], dy[D], du[D];
-    cell_derivs<D, LX>(fy, sm + T::E + w0, sm + T::V + w0, lL, lR, dx);    // flux_y
-    cell_derivs<D, LX>(dy, sm + T::PGV + w0, sm + T::PG + w0, lL, lR, dx); // div_y
-    cell_derivs<D, LX>(du, sm + T::U + w0, sm + T::U + w0, sL, sR, dx);    // dudy
-    const int mmax = (c == ncy - 1 && last_y) ? D : D - 1;
-#pragma unroll
-    for (int m = 0; m < D; ++m) {
-      if (m >= mmax) continue;
-      const int r = c * (D - 1) + m;
-      const int sidx = (r + H) * LX + (q + H);
-      const double sg = sm[T::SG + sidx], cu = sm[T::CU + sidx], cv = sm[T::CV + sidx];
-      const long long go = (long long)(Y0 + H + r) * g.P + (X0 + H + q);
-      const double fc = __ldg(a.fcor + pbase + go);
-      const double *xr = sm + T::XR + r * T::TX + q;
-      const double flux_x = xr[0], div_x = xr[T::TY * T::TX], dvdx = xr[2 * T::TY * T::TX];
-      const double vort = (dvdx - du[m]) / sg;
-      const double tP = -div_x - dy[m];
-      const double tU = -flux_x + sg * (vort + fc) * cv;
-      const double tV = -fy[m] - sg * (vort + fc) * cu;
-      const double us = sm[T::U + sidx], vs = sm[T::V + sidx], pgs = sm[T::PG + sidx];
-      double uo, vo, pgo;
-      if constexpr (KIND == RK3_S1 || KIND == RK4_S1) {
-        uo = us + a.inc * tU;
-        vo = vs + a.inc * tV;
-        pgo = pgs + a.inc * tP;
-        if constexpr (KIND == RK4_S1) {
-          a.aU[mbase + go] = tU;
-          a.aV[mbase + go] = tV;
-          a.aP[mbase + go] = tP;
-        }
-      } else {
-        const double ub = a.u0[mbase + go], vb = a.v0[mbase + go], pgb = a.p0[mbase + go] * sg;
-        if constexpr (KIND == RK4_S2 || KIND == RK4_S3) {
-          uo = ub + a.inc * tU;
-          vo = vb + a.inc * tV;
-          pgo = pgb + a.inc * tP;
-          a.aU[mbase + go] = a.aU[mbase + go] + 2. * tU;
-          a.aV[mbase + go] = a.aV[mbase + go] + 2. * tV;
-          a.aP[mbase + go] = a.aP[mbase + go] + 2. * tP;
-        } else if constexpr (KIND == RK4_S4) {
-          uo = ub + a.inc * ((a.aU[mbase + go] + tU) / 6.);
-          vo = vb + a.inc * ((a.aV[mbase + go] + tV) / 6.);
-          pgo = pgb + a.inc * ((a.aP[mbase + go] + tP) / 6.);
-        } else if constexpr (KIND == RK3_S2) {
-          uo = 0.75 * ub + 0.25 * us + a.inc * tU;
-          vo = 0.75 * vb + 0.25 * vs + a.inc * tV;
-          pgo = 0.75 * pgb + 0.25 * pgs + a.inc * tP;
-        } else {  // RK3_S3
-          uo = ub / 3. + 2. / 3. * us + a.inc * tU;
-          vo = vb / 3. + 2. / 3. * vs + a.inc * tV;
-          pgo = pgb / 3. + 2. / 3. * pgs + a.inc * tP;
-        }
+  const int qown = last_x ? txe : txe - 1;  // seam points belong to the left / lower tile
+  const int rown = last_y ? tye : tye - 1;
+  for (int it = threadIdx.x; it < T::I; it += NT) {
+    const int r = it / T::TX, q = it - r * T::TX;
+    if (q >= qown || r >= rown) continue;
+    const long long go = (long long)(Y0 + H + r) * g.P + (X0 + H + q);
+    const double fc = __ldg(a.fcor + pbase + go);
+    double ub = 0., vb = 0., pb = 0., aU = 0., aV = 0., aP = 0.;
+    if constexpr (KIND != RK3_S1 && KIND != RK4_S1) {
+      ub = a.u0[mbase + go];
+      vb = a.v0[mbase + go];
+      pb = a.p0[mbase + go];
+    }
+    if constexpr (KIND == RK4_S2 || KIND == RK4_S3 || KIND == RK4_S4) {
+      aU = a.aU[mbase + go];
+      aV = a.aV[mbase + go];
+      aP = a.aP[mbase + go];
+    }
+    const int sidx = (r + H) * LX + (q + H);
+    const int ridx = r * T::TX + q;
+    const double sg = sm[T::SG + sidx], cu = sm[T::CU + sidx], cv = sm[T::CV + sidx];
+    const double rsg = 1. / sg;
+    const double flux_x = sm[T::XR + ridx], div_x = sm[T::XR + T::I + ridx], dvdx = sm[T::XR + 2 * T::I + ridx];
+    const double flux_y = sm[T::YR + ridx], div_y = sm[T::YR + T::I + ridx], dudy = sm[T::YR + 2 * T::I + ridx];
+    const double vort = (dvdx - dudy) * rsg;
+    const double tP = -div_x - div_y;
+    const double tU = -flux_x + sg * (vort + fc) * cv;
+    const double tV = -flux_y - sg * (vort + fc) * cu;
+    const double us = sm[T::U + sidx], vs = sm[T::V + sidx], pgs = sm[T::PG + sidx];
+    double uo, vo, pgo;
+    if constexpr (KIND == RK3_S1 || KIND == RK4_S1) {
+      uo = us + a.inc * tU;
+      vo = vs + a.inc * tV;
+      pgo = pgs + a.inc * tP;
+      if constexpr (KIND == RK4_S1) {
+        a.aU[mbase + go] = tU;
+        a.aV[mbase + go] = tV;
+        a.aP[mbase + go] = tP;
       }
-      const double po = pgo / sg;  // time_scheme_mod.F90:81
-      a.uo[mbase + go] = uo;
-      a.vo[mbase + go] = vo;
-      a.po[mbase + go] = po;
-      const int gi = X0 + q, gj = Y0 + r;  // 0-based interior indices
-      const int nn = g.n;
-      if (gi == 0 || gi == nn - 1 || gj == 0 || gj == nn - 1) {
-        // pre-unification boundary values for the halo kernel
-        const double4 val = make_double4(uo, vo, po, 0.);
-        double4 *b = a.bnd + ((long long)mem * 6 + panel) * 4 * nn;
-        if (gi == 0) b[0 * nn + gj] = val;
-        if (gi == nn - 1) b[1 * nn + gj] = val;
-        if (gj == 0) b[2 * nn + gi] = val;
-        if (gj == nn - 1) b[3 * nn + gi] = val;
+    } else {
+      const double pgb = pb * sg;
+      if constexpr (KIND == RK4_S2 || KIND == RK4_S3) {
+        uo = ub + a.inc * tU;
+        vo = vb + a.inc * tV;
+        pgo = pgb + a.inc * tP;
+        a.aU[mbase + go] = aU + 2. * tU;
+        a.aV[mbase + go] = aV + 2. * tV;
+        a.aP[mbase + go] = aP + 2. * tP;
+      } else if constexpr (KIND == RK4_S4) {
+        uo = ub + a.inc * ((aU + tU) * (1. / 6.));
+        vo = vb + a.inc * ((aV + tV) * (1. / 6.));
+        pgo = pgb + a.inc * ((aP + tP) * (1. / 6.));
+      } else if constexpr (KIND == RK3_S2) {
+        uo = 0.75 * ub + 0.25 * us + a.inc * tU;
+        vo = 0.75 * vb + 0.25 * vs + a.inc * tV;
+        pgo = 0.75 * pgb + 0.25 * pgs + a.inc * tP;
+      } else {  // RK3_S3
+        uo = ub * (1. / 3.) + 2. / 3. * us + a.inc * tU;
+        vo = vb * (1. / 3.) + 2. / 3. * vs + a.inc * tV;
+        pgo = pgb * (1. / 3.) + 2. / 3. * pgs + a.inc * tP;
       }
+    }
+    const double po = pgo * rsg;  // phi = phiG / sqrtG, time_scheme_mod.F90:81
+    a.uo[mbase + go] = uo;
+    a.vo[mbase + go] = vo;
+    a.po[mbase + go] = po;
+    const int gi = X0 + q, gj = Y0 + r;  // 0-based interior indices
+    const int nn = g.n;
+    if (gi == 0 || gi == nn - 1 || gj == 0 || gj == nn - 1) {
+      // pre-unification boundary values for the halo kernel
+      const double4 val = make_double4(uo, vo, po, 0.);
+      double4 *b = a.bnd + ((long long)mem * 6 + panel) * 4 * nn;
+      if (gi == 0) b[0 * nn + gj] = val;
+      if (gi == nn - 1) b[1 * nn + gj] = val;
+      if (gj == 0) b[2 * nn + gi] = val;
+      if (gj == nn - 1) b[3 * nn + gi] = val;
     }
   }
 }
@@ -369,21 +400,26 @@ template <int D>
 __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloArgs a) {
   constexpr int H = D - 1;
   const int n = g.n;
+  // one thread per (member, panel, edge, halo line h = 0..H, position k)
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long per_member = 24LL * n;
+  const long long per_member = 24LL * (H + 1) * n;
   if (gid >= per_member * a.members) return;
   const int mem = (int)(gid / per_member);
-  const int rem = (int)(gid - (long long)mem * per_member);
-  const int p = rem / (4 * n), e = (rem / n) % 4, k = rem % n;
+  int rem = (int)(gid - (long long)mem * per_member);
+  const int k = rem % n;
+  rem /= n;
+  const int h = rem % (H + 1);
+  const int pe = rem / (H + 1);
+  const int p = pe / 4, e = pe % 4;
   const EdgeLink L = c_links[p][e];
   const int q = L.q, e2 = L.e2;
   const long long mb = (long long)mem * g.mstride;
   const double4 *bnd_m = a.bnd + (long long)mem * 24 * n;
 
-  // halo lines h = 1..H: neighbour line h rotated to the sphere, interpolated
-  // along the edge, rotated back to this panel (ghost_mod.f90:154-181)
-#pragma unroll
-  for (int h = 1; h <= H; ++h) {
+  double zw, mw, ph;
+  if (h > 0) {
+    // halo line h: neighbour line h rotated to the sphere, interpolated along
+    // the edge, rotated back to this panel (ghost_mod.f90:154-181)
     const int iref = a.giref[(h - 1) * n + k];
     const double2 cc = a.gcoef[(h - 1) * n + k];
     double qz[D], qm[D], qp[D];
@@ -406,21 +442,11 @@ __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloA
       qm[m] = M.y * su + M.w * sv;
       qp[m] = sp;
     }
-    const double zw = ghost_interp<D>(qz, cc.x, cc.y, a.dx, a.dx2, a.dx3);
-    const double mw = ghost_interp<D>(qm, cc.x, cc.y, a.dx, a.dx2, a.dx3);
-    const double ph = ghost_interp<D>(qp, cc.x, cc.y, a.dx, a.dx2, a.dx3);
-    const double4 N = a.Ntab[((p * 4 + e) * (H + 1) + h) * n + k];
-    int di, dj;
-    strip_point(e, -h, k, n, di, dj);
-    const long long o = mb + p * g.plane + (long long)(dj + H) * g.P + (di + H);
-    a.u[o] = N.x * zw + N.z * mw;  // covProjSphere2Plane, projection_mod.F90:60-77
-    a.v[o] = N.y * zw + N.w * mw;
-    a.phi[o] = ph;
-  }
-
-  // boundary line: unify (spatial_operators_mod.F90:282-388) and SP2P (:459-492)
-  double zw, mw, ph;
-  if (k > 0 && k < n - 1) {
+    zw = ghost_interp<D>(qz, cc.x, cc.y, a.dx, a.dx2, a.dx3);
+    mw = ghost_interp<D>(qm, cc.x, cc.y, a.dx, a.dx2, a.dx3);
+    ph = ghost_interp<D>(qp, cc.x, cc.y, a.dx, a.dx2, a.dx3);
+  } else if (k > 0 && k < n - 1) {
+    // boundary line: edge average (spatial_operators_mod.F90:298-345)
     const int ks = L.rev ? n - 1 - k : k;
     const double4 bo = bnd_m[(p * 4 + e) * n + k];
     const double4 bn = bnd_m[(q * 4 + e2) * n + ks];
@@ -430,7 +456,7 @@ __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloA
     mw = 0.5 * ((Mo.y * bo.x + Mo.w * bo.y) + (Mn.y * bn.x + Mn.w * bn.y));
     ph = 0.5 * (bo.z + bn.z);
   } else if (e <= 1) {
-    // cube vertex, owned by the W/E edge threads
+    // cube vertex (:347-386), owned by the W/E edge threads
     const int corner = (e == 0) ? (k == 0 ? 0 : 2) : (k == 0 ? 1 : 3);
     const VertexRef V = c_vertex[p][corner];
     double z[3], mm[3], pp[3];
@@ -451,9 +477,10 @@ __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloA
   } else {
     return;
   }
-  const double4 N = a.Ntab[((p * 4 + e) * (H + 1) + 0) * n + k];
+  // back to this panel's covariant winds (covProjSphere2Plane, :459-492)
+  const double4 N = a.Ntab[((p * 4 + e) * (H + 1) + h) * n + k];
   int di, dj;
-  strip_point(e, 0, k, n, di, dj);
+  strip_point(e, -h, k, n, di, dj);
   const long long o = mb + p * g.plane + (long long)(dj + H) * g.P + (di + H);
   a.u[o] = N.x * zw + N.z * mw;
   a.v[o] = N.y * zw + N.w * mw;
