@@ -40,7 +40,8 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=["large", "small", "stress"], default="large")
-    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    p.add_argument("--error-days", type=float, default=5.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=5)
     return p.parse_args()
@@ -67,13 +68,21 @@ def build_workload(name):
     return st, geom, desc
 
 
-def stage_words(scheme, precision):
-    """Algorithmic 8-byte words per interior PV per stage: stage input (3),
-    RK base where the stage reads it (3), 6 metric scalars, stage output (3),
-    RK4 accumulator read/write (3 each)."""
+def stage_bytes(scheme, precision):
+    """Algorithmic bytes per interior PV of each stage-kernel launch.
+
+    FP64: 8-byte words of stage input (3), RK base where the stage reads it (3),
+    6 metric scalars, stage output (3), RK4 accumulator read/write (3 each):
+    RK3 12, 15, 15 words; RK4 15, 21, 21, 18.
+    Split precision: FP64 state (24 B), FP32 input increment (12), FP32 phi_s
+    (4; the metric is recomputed from 1-D tables), FP32 output increment (12) or
+    FP64 new state (24), FP32 RK4 accumulator read/write (12 each)."""
+    if precision == "fp64":
+        words = [12, 15, 15] if scheme == "RK3_TVD" else [15, 21, 21, 18]
+        return [8 * w for w in words]
     if scheme == "RK3_TVD":
-        return [12, 15, 15]
-    return [15, 21, 21, 18]
+        return [24 + 4 + 12, 24 + 12 + 4 + 12, 24 + 12 + 4 + 24]
+    return [24 + 4 + 12 + 12, 24 + 12 + 4 + 12 + 24, 24 + 12 + 4 + 12 + 24, 24 + 12 + 4 + 12 + 24]
 
 
 class ClockSampler:
@@ -193,30 +202,14 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
+def time_path(args, st, geom, precision, world, barrier, dist, local):
+    """Device time of args.steps RK steps of one precision (state resident)."""
     import torch
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
     from mcv_sw_b200 import api
-    st, geom, desc = build_workload(args.workload)
     n_pv = 6 * geom.n * geom.n
-
-    s = api.Stepper(st.order, st.nc, st.dt, st.scheme, members=1, precision=args.precision,
-                    radius=6.371e6)
+    s = api.Stepper(st.order, st.nc, st.dt, st.scheme, members=1, precision=precision, radius=6.371e6)
     s.set_geometry(geom)
     s.set_member(0, st.phi_s, st.u, st.v, st.phi)
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
     s.time_steps(max(args.warmup, 3))
     barrier()
     clocks = ClockSampler(local)
@@ -228,38 +221,70 @@ def run_ours(args):
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    sim_days = args.steps * st.dt / 86400.0
-    value = world * sim_days / (ms / 1e3)
-
-    # roofline of the fused stage kernel: algorithmic bytes / launch time
+    value = world * args.steps * st.dt / 86400.0 / (ms / 1e3)
     stage_ms, halo_ms = s.profile_step(3)
-    words = stage_words(st.scheme, args.precision)
-    alg_bytes = [w * 8 * n_pv for w in words]
-    achieved = sum(alg_bytes) / (sum(stage_ms) * 1e-3) / 1e9
+    per_pv = stage_bytes(st.scheme, precision)
+    achieved = sum(b * n_pv for b in per_pv) / (sum(stage_ms) * 1e-3) / 1e9
+    cands, chosen = s.tuning()
+    out = {"value": value, "ms_per_step": ms / args.steps, "stage_ms": stage_ms, "halo_ms": halo_ms,
+           "achieved_gbs": achieved, "bytes_per_pv_step": sum(per_pv), "clocks": clk,
+           "tile": {"chosen_cells_threads": list(cands[chosen][0]),
+                    "candidates": [{"cells_threads": list(c), "ms": round(t, 5)} for c, t in cands]}}
+    return s, out
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from mcv_sw_b200 import api, diag
+    st, geom, desc = build_workload(args.workload)
+    n_pv = 6 * geom.n * geom.n
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    paths = {}
+    for precision in ("fp64", "mixed"):
+        s, paths[precision] = time_path(args, st, geom, precision, world, barrier, dist, local)
+        if precision != args.precision:
+            s.close()
+        else:
+            main = s
+    head = paths[args.precision]
     peak, peak_kind = measured_peak()
     traffic_pv = stage_traffic_per_pv()
     key = (args.workload, f"{st.scheme}-{args.precision}")
     traffic = traffic_pv[key] * n_pv if key in traffic_pv else None
-    step_ms = ms / args.steps
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": peak_kind, "kernel": "stage_kernel",
-                "algorithmic_bytes_per_launch": sum(alg_bytes) / len(alg_bytes),
-                "stage_ms": stage_ms, "halo_ms": halo_ms,
-                "halo_share_of_step": len(stage_ms) * halo_ms / step_ms}
+    nst = len(head["stage_ms"])
+    roofline = {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                "frac": head["achieved_gbs"] / peak, "traffic": traffic, "peak_source": peak_kind,
+                "kernel": f"stage_kernel ({args.precision})",
+                "algorithmic_bytes_per_launch": head["bytes_per_pv_step"] * n_pv / nst,
+                "stage_ms": head["stage_ms"], "halo_ms": head["halo_ms"],
+                "halo_share_of_step": nst * head["halo_ms"] / head["ms_per_step"]}
 
     # end to end through the C ABI with pinned host buffers: per step upload the
     # state, advance one RK step, download the state
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     hp = {k: pin(getattr(st, k)) for k in ("phi_s", "u", "v", "phi")}
     ho = {k: torch.empty(geom.shape, dtype=torch.float64).pin_memory().numpy() for k in ("u", "v", "phi")}
-    s.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
-    s.step(1)
+    main.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
+    main.step(1)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        s.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
-        s.step(1)
-        s.get_state(0, out=ho)
+        main.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
+        main.step(1)
+        main.get_state(0, out=ho)
     barrier()
     e2e_s = time.perf_counter() - t0
     if dist is not None:
@@ -271,22 +296,45 @@ def run_ours(args):
            "h2d_bytes_per_step": 4 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
            "how": "per step: mcv_set_member (phi_s, u, v, phi from pinned host) + mcv_step(1) + "
                   "mcv_get_state (u, v, phi to pinned host); host wall clock around synchronous calls"}
-    s.close()
+    main.close()
+
+    # accuracy of split precision against the FP64 path over the full forecast
+    accuracy = None
+    if rank == 0 and args.error_days > 0:
+        nsteps = int(round(args.error_days * 86400.0 / st.dt))
+        finals, drift = {}, {}
+        for precision in ("fp64", "mixed"):
+            with api.Stepper(st.order, st.nc, st.dt, st.scheme, precision=precision, radius=6.371e6) as s:
+                s.set_geometry(geom)
+                s.set_member(0, st.phi_s, st.u, st.v, st.phi)
+                m0, _ = s.mass_energy(0)
+                s.step(nsteps)
+                m1, _ = s.mass_energy(0)
+                finals[precision] = s.get_state(0)["phi"] / 9.80616
+                drift[precision] = (m1 - m0) / m0
+        l1, l2, linf = diag.norms(geom, finals["mixed"], finals["fp64"])
+        accuracy = {"sim_days": nsteps * st.dt / 86400.0, "steps": nsteps,
+                    "height_error_vs_fp64": {"L1": l1, "L2": l2, "Linf": linf},
+                    "mass_drift": drift, "reference": "FP64 GPU path (oracle-validated by the parity tests)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(st)
     if rank == 0:
-        stages = len(words)
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+        other = "fp64" if args.precision == "mixed" else "mixed"
+        line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
                 "config": {"workload": desc, "order": st.order, "nc": st.nc, "scheme": st.scheme,
                            "precision": args.precision, "dt_s": st.dt, "interior_pvs": n_pv,
                            "parallelism": f"replicas{world}",
                            "l2": "no flush: each stage reads > 126 MB (inputs larger than L2)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": args.steps * 2 * stages, "clocks": clk}
+                "gpu_launches": args.steps * 2 * nst, "clocks": head["clocks"],
+                "paths": {"fp64": paths["fp64"], "mixed": paths["mixed"]},
+                f"speedup_{args.precision}_vs_{other}": head["value"] / paths[other]["value"],
+                "accuracy": accuracy}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -104,6 +104,17 @@ int mcv_mass_energy(mcv_handle *h, int m, double *mass, double *energy);
 int mcv_time_steps(mcv_handle *h, int nsteps, double *ms);
 int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, double *halo_ms);
 
+/* Stage-kernel tile shapes the autotuner timed on this handle's grid (it runs
+ * once, before the first step): ncand candidates, shapes[3*i..] = {cells in x,
+ * cells in y, threads}, ms[i] = device time per launch, *chosen = the index in
+ * use.  No counterpart in the reference (which has no GPU path). */
+int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, float *ms);
+
+/* Use candidate `index` of mcv_tuning's list instead of the autotuner's choice
+ * (-1 re-runs the autotuner before the next step).  The tile shape changes the
+ * schedule, not the arithmetic: every shape gives bit-identical states. */
+int mcv_select_tile(mcv_handle *h, int index);
+
 /* Release the handle and its device memory. */
 int mcv_destroy(mcv_handle *h);
 

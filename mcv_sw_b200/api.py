@@ -60,6 +60,8 @@ def lib():
         "mcv_destroy": (ctypes.c_int, [vp]),
         "mcv_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _D]),
         "mcv_profile_step": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
+        "mcv_tuning": (ctypes.c_int, [vp, _I, _I, _I, ctypes.POINTER(ctypes.c_float)]),
+        "mcv_select_tile": (ctypes.c_int, [vp, ctypes.c_int]),
         "mcv_grid_sizes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _I, _I, _I]),
         "mcv_footprint_bytes": (ctypes.c_longlong, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_int]),
@@ -263,6 +265,18 @@ class Stepper:
         _check(lib().mcv_profile_step(self.h, int(nsteps), st, ctypes.byref(ha)))
         nst = 3 if self.scheme == "RK3_TVD" else 4
         return list(st)[:nst], ha.value
+
+    def tuning(self):
+        """Autotuner record: list of ((cells_x, cells_y, threads), ms per launch) and the chosen index."""
+        n, ch = ctypes.c_int(), ctypes.c_int()
+        shapes = (ctypes.c_int * 48)()
+        ms = (ctypes.c_float * 16)()
+        _check(lib().mcv_tuning(self.h, ctypes.byref(n), ctypes.byref(ch), shapes, ms))
+        cands = [((shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]), ms[i]) for i in range(n.value)]
+        return cands, ch.value
+
+    def select_tile(self, index):
+        _check(lib().mcv_select_tile(self.h, int(index)))
 
     def mass_energy(self, m=0):
         ms, en = ctypes.c_double(), ctypes.c_double()

@@ -10,8 +10,10 @@ LIB_PATH = os.path.join(LIB_DIR, "libmcv_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
-SOURCES = ["mcv_gpu.cu", "host_setup.cpp"]
-HEADERS = ["mcv_kernels.cuh", "mcv_internal.h", os.path.join("..", "..", "include", "mcv_gpu.h")]
+SOURCES = ["mcv_gpu.cu", "stage_d3_f64.cu", "stage_d3_mix.cu", "stage_d4_f64.cu", "stage_d4_mix.cu",
+           "host_setup.cpp"]
+HEADERS = ["mcv_stage.cuh", "mcv_halo.cuh", "mcv_internal.h", os.path.join("..", "..", "include", "mcv_gpu.h")]
+OBJ_DIR = os.path.join(HERE, "_lib", "obj")
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",
@@ -19,7 +21,6 @@ NVCC_FLAGS = [
     "-lineinfo",
     "-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off,-O2",
     "-ccbin", HOST_CXX,
-    "-shared",
 ]
 
 
@@ -32,14 +33,24 @@ def _stale():
 
 
 def build(force=False, verbose=False, extra_flags=()):
-    """Compile the CUDA/C++ library; returns its path."""
+    """Compile the CUDA/C++ library (one object per source, in parallel); returns its path."""
     if not force and not _stale():
         return LIB_PATH
-    os.makedirs(LIB_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+        objs.append(obj)
+        cmd = [NVCC] + NVCC_FLAGS + list(extra_flags) + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((src, subprocess.Popen(cmd)))
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed on {failed}")
     tmp = LIB_PATH + ".tmp"
-    cmd = [NVCC] + NVCC_FLAGS + list(extra_flags) + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lgomp"]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
+    cmd = [NVCC, "-shared", "-ccbin", HOST_CXX, "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + [
+        "-lgomp"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH

@@ -2,7 +2,9 @@
 //
 // A handle holds one grid (order, Nc) and `members` states, all resident in
 // HBM.  One RK step is 2 * stages kernel launches (fused stage K1, halo K2),
-// captured once into a CUDA graph and replayed per step.
+// captured into a CUDA graph and replayed per step.  The stage kernel's tile
+// shape is chosen per handle by timing every candidate shape on the handle's
+// own grid before the first step (the autotuner).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -12,8 +14,8 @@
 #include <vector>
 
 #include "../../include/mcv_gpu.h"
+#include "mcv_halo.cuh"
 #include "mcv_internal.h"
-#include "mcv_kernels.cuh"
 
 namespace mcv {
 
@@ -30,11 +32,21 @@ static int cuda_fail(cudaError_t e, const char *what) {
   return (e == cudaErrorMemoryAllocation) ? MCV_ERR_NOMEM : MCV_ERR_CUDA;
 }
 
-#define MCV_CUDA(call, what)                      \
-  do {                                            \
-    cudaError_t _e = (call);                      \
+#define MCV_CUDA(call, what)                           \
+  do {                                                 \
+    cudaError_t _e = (call);                           \
     if (_e != cudaSuccess) return cuda_fail(_e, what); \
   } while (0)
+
+const StageLauncher *stage_launchers_d3_f64(int *count);
+const StageLauncher *stage_launchers_d3_mix(int *count);
+const StageLauncher *stage_launchers_d4_f64(int *count);
+const StageLauncher *stage_launchers_d4_mix(int *count);
+
+const StageLauncher *stage_launchers(int order, bool mixed, int *count) {
+  if (order == 3) return mixed ? stage_launchers_d3_mix(count) : stage_launchers_d3_f64(count);
+  return mixed ? stage_launchers_d4_mix(count) : stage_launchers_d4_f64(count);
+}
 
 // Cube connectivity from CubedSphereFillHalo (src/ghost_mod.f90:104-146):
 // {neighbour panel, neighbour edge, reversed}, panels 0-based, edges W E S N.
@@ -80,17 +92,8 @@ static int upload_tables() {
   return MCV_OK;
 }
 
-// Tile shapes (cells) of the stage kernel per order.
-template <int D>
-struct TileShape;
-template <>
-struct TileShape<3> {
-  static constexpr int CX = 12, CY = 12, NT = 320;
-};
-template <>
-struct TileShape<4> {
-  static constexpr int CX = 8, CY = 8, NT = 320;
-};
+constexpr double kOmega = 7.292E-5;  // constants_mod.F90:18
+constexpr int kPartialBlocks = 296;
 
 }  // namespace mcv
 
@@ -98,6 +101,7 @@ using namespace mcv;
 
 struct mcv_handle {
   int order = 0, nc = 0, scheme = 0, precision = 0, members = 0;
+  bool mixed = false;
   double dt = 0, radius = 0;
   GridDesc g{};
   int H = 0, npx = 0;
@@ -106,7 +110,18 @@ struct mcv_handle {
   // device memory (one allocation)
   void *pool = nullptr;
   size_t pool_bytes = 0;
+  // FP64 policy: state Y, stage buffers A, B, RK4 accumulator
   double *Y[3]{}, *A[3]{}, *B[3]{}, *acc[3]{};
+  // split precision: FP64 state ping-pong S[cur], S[1-cur]; FP32 increments DA, DB
+  double *S[2][3]{};
+  int cur = 0;
+  float *DA[3]{}, *DB[3]{}, *facc[3]{};
+  float *phis32 = nullptr;
+  float4 *bnd32 = nullptr;
+  double4 *met1d = nullptr;
+  double *phibar = nullptr;
+  std::vector<double> phibar_host;
+  // shared
   double *sqrtG = nullptr, *ig11 = nullptr, *ig12 = nullptr, *ig22 = nullptr, *fcor = nullptr, *phis = nullptr;
   double4 *bnd = nullptr, *Mtab = nullptr, *Ntab = nullptr;
   int *giref = nullptr;
@@ -117,20 +132,14 @@ struct mcv_handle {
   std::vector<char> member_set;
   std::vector<long long> steps_done;
   std::vector<double> sqrtG_host;  // padded Fortran layout, for phiG on download
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
+  // stage kernel chosen by the autotuner
+  const StageLauncher *cands = nullptr;
+  int ncands = 0, choice = -1;
+  std::vector<float> tune_ms;
+  cudaGraphExec_t graph_exec[2]{};
 };
 
 namespace {
-
-constexpr int kPartialBlocks = 296;
-
-struct Layout {
-  size_t field;   // bytes of one padded field for all members
-  size_t plane6;  // bytes of one padded field of one member (6 panels)
-  size_t total;
-  size_t off_state[9], off_acc[3], off_metric[5], off_phis, off_bnd, off_M, off_N, off_iref, off_coef, off_partial;
-};
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -145,36 +154,58 @@ void grid_desc(int order, int nc, GridDesc &g, int &H, int &npx) {
   g.mstride = 6 * g.plane;
 }
 
-Layout make_layout(const GridDesc &g, int H, int scheme, int members) {
-  Layout L{};
-  L.plane6 = (size_t)g.mstride * sizeof(double);
-  L.field = L.plane6 * members;
+// Offsets of every device array inside the handle's single allocation.
+struct Layout {
+  size_t total = 0;
+  size_t f64_state[9]{}, f64_acc[3]{}, mix_state[6]{}, mix_inc[6]{}, mix_acc[3]{};
+  size_t metric[5]{}, phis = 0, phis32 = 0, bnd = 0, bnd32 = 0, M = 0, N = 0, iref = 0, coef = 0, partial = 0,
+         met1d = 0, phibar = 0;
+};
+
+Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int members) {
+  Layout L;
+  const size_t f64 = (size_t)g.mstride * sizeof(double) * members;  // one FP64 padded field, all members
+  const size_t f32 = (size_t)g.mstride * sizeof(float) * members;
+  const size_t plane6 = (size_t)g.mstride * sizeof(double);
   size_t off = 0;
   auto take = [&](size_t bytes) {
     size_t o = off;
     off = align_up(off + bytes, 256);
     return o;
   };
-  for (int k = 0; k < 9; ++k) L.off_state[k] = take(L.field);
-  for (int k = 0; k < 3; ++k) L.off_acc[k] = (scheme == MCV_RK4) ? take(L.field) : 0;
-  for (int k = 0; k < 5; ++k) L.off_metric[k] = take(L.plane6);
-  L.off_phis = take(L.field);
-  L.off_bnd = take(sizeof(double4) * 24 * (size_t)g.n * members);
-  L.off_M = take(sizeof(double4) * 24 * (size_t)(H + 1) * g.n);
-  L.off_N = take(sizeof(double4) * 24 * (size_t)(H + 1) * g.n);
-  L.off_iref = take(sizeof(int) * (size_t)H * g.n);
-  L.off_coef = take(sizeof(double2) * (size_t)H * g.n);
-  L.off_partial = take(sizeof(double4) * kPartialBlocks);
+  const bool rk4 = scheme == MCV_RK4;
+  if (precision == MCV_FP64) {
+    for (int k = 0; k < 9; ++k) L.f64_state[k] = take(f64);
+    if (rk4)
+      for (int k = 0; k < 3; ++k) L.f64_acc[k] = take(f64);
+  } else {
+    for (int k = 0; k < 6; ++k) L.mix_state[k] = take(f64);
+    for (int k = 0; k < 6; ++k) L.mix_inc[k] = take(f32);
+    if (rk4)
+      for (int k = 0; k < 3; ++k) L.mix_acc[k] = take(f32);
+    L.phis32 = take(f32);
+    L.bnd32 = take(sizeof(float4) * 24 * (size_t)g.n * members);
+    L.met1d = take(sizeof(double4) * (size_t)g.np);
+    L.phibar = take(sizeof(double) * members);
+  }
+  for (int k = 0; k < 5; ++k) L.metric[k] = take(plane6);
+  L.phis = take(f64);
+  L.bnd = take(sizeof(double4) * 24 * (size_t)g.n * members);
+  L.M = take(sizeof(double4) * 24 * (size_t)(H + 1) * g.n);
+  L.N = take(sizeof(double4) * 24 * (size_t)(H + 1) * g.n);
+  L.iref = take(sizeof(int) * (size_t)H * g.n);
+  L.coef = take(sizeof(double2) * (size_t)H * g.n);
+  L.partial = take(sizeof(double4) * kPartialBlocks);
   L.total = off;
   return L;
 }
 
 // Copy a host array in the reference's padded Fortran layout (npx*npx*6,
-// contiguous) into the pitched device layout of member slot `dst`.
-int upload_padded(mcv_handle *h, double *dst, const double *src) {
-  const size_t row = (size_t)h->npx * sizeof(double);
-  MCV_CUDA(cudaMemcpy2DAsync(dst, (size_t)h->g.P * sizeof(double), src, row, row, (size_t)h->npx * 6,
-                             cudaMemcpyHostToDevice, h->stream),
+// contiguous) into the pitched device layout.
+int upload_padded(mcv_handle *h, void *dst, const void *src, size_t elem) {
+  const size_t row = (size_t)h->npx * elem;
+  MCV_CUDA(cudaMemcpy2DAsync(dst, (size_t)h->g.P * elem, src, row, row, (size_t)h->npx * 6, cudaMemcpyHostToDevice,
+                             h->stream),
            "upload field");
   return MCV_OK;
 }
@@ -187,40 +218,67 @@ int download_padded(mcv_handle *h, double *dst, const double *src) {
   return MCV_OK;
 }
 
-template <int D, int KIND>
-void launch_stage(mcv_handle *h, const StageArgs &a) {
-  using S = TileShape<D>;
-  using T = Tile<D, S::CX, S::CY>;
-  dim3 grid(h->g.tiles_x * h->g.tiles_y, 6, h->members);
-  stage_kernel<D, S::CX, S::CY, S::NT, KIND><<<grid, S::NT, T::BYTES, h->stream>>>(h->g, a);
+int num_stages(const mcv_handle *h) { return h->scheme == MCV_RK3_TVD ? 3 : 4; }
+
+// Stage kind of stage s of the handle's scheme.
+int stage_kind(const mcv_handle *h, int s) { return (h->scheme == MCV_RK3_TVD ? RK3_S1 : RK4_S1) + s; }
+
+// Stage arguments of stage s of one RK step.  FP64: the buffer sequence of
+// RK3_TVD / RK4 (src/time_scheme_mod.F90:13-69) with the last stage writing Y
+// in place.  Split precision: stages carry FP32 increments over the FP64 state
+// S[c]; the last stage writes S[1-c].
+StageArgs stage_args(mcv_handle *h, int s, int c) {
+  StageArgs a{};
+  a.sqrtG = h->sqrtG; a.ig11 = h->ig11; a.ig12 = h->ig12; a.ig22 = h->ig22; a.fcor = h->fcor;
+  a.phis = h->phis;
+  a.bnd = h->bnd;
+  const double dt = h->dt;
+  const int kind = stage_kind(h, s);
+  if (!h->mixed) {
+    a.aU = h->acc[0]; a.aV = h->acc[1]; a.aP = h->acc[2];
+    double *const *in, *const *out;
+    double inc;
+    switch (kind) {
+      case RK3_S1: in = h->Y; out = h->A; inc = dt; break;
+      case RK3_S2: in = h->A; out = h->B; inc = 0.25 * dt; break;
+      case RK3_S3: in = h->B; out = h->Y; inc = 2. / 3. * dt; break;
+      case RK4_S1: in = h->Y; out = h->A; inc = 0.5 * dt; break;
+      case RK4_S2: in = h->A; out = h->B; inc = 0.5 * dt; break;
+      case RK4_S3: in = h->B; out = h->A; inc = dt; break;
+      default: in = h->A; out = h->Y; inc = dt; break;
+    }
+    a.us = in[0]; a.vs = in[1]; a.ps = in[2];
+    a.u0 = h->Y[0]; a.v0 = h->Y[1]; a.p0 = h->Y[2];
+    a.uo = out[0]; a.vo = out[1]; a.po = out[2];
+    a.inc = inc;
+    return a;
+  }
+  double *const *Y = h->S[c], *const *Yn = h->S[1 - c];
+  a.yu = Y[0]; a.yv = Y[1]; a.yp = Y[2];
+  a.uo = Yn[0]; a.vo = Yn[1]; a.po = Yn[2];
+  a.fU = h->facc[0]; a.fV = h->facc[1]; a.fP = h->facc[2];
+  a.phis32 = h->phis32; a.met1d = h->met1d; a.phibar = h->phibar; a.bnd32 = h->bnd32;
+  a.two_omega = 2. * kOmega;
+  float *const *din = nullptr, *const *dout = nullptr;
+  float wd = 0.f, wt = 0.f;
+  switch (kind) {
+    case RK3_S1: dout = h->DA; wt = (float)dt; break;
+    case RK3_S2: din = h->DA; dout = h->DB; wd = 0.25f; wt = (float)(0.25 * dt); break;
+    case RK3_S3: din = h->DB; wd = (float)(2. / 3.); wt = (float)(2. / 3. * dt); break;
+    case RK4_S1: dout = h->DA; wt = (float)(0.5 * dt); break;
+    case RK4_S2: din = h->DA; dout = h->DB; wt = (float)(0.5 * dt); break;
+    case RK4_S3: din = h->DB; dout = h->DA; wt = (float)dt; break;
+    default: din = h->DA; wt = (float)dt; break;
+  }
+  if (din) { a.du = din[0]; a.dv = din[1]; a.dp = din[2]; }
+  if (dout) { a.eu = dout[0]; a.ev = dout[1]; a.ep = dout[2]; }
+  a.wd = wd;
+  a.wt = wt;
+  return a;
 }
 
-template <int D>
-int prepare_kernels() {
-  using S = TileShape<D>;
-  using T = Tile<D, S::CX, S::CY>;
-  const int bytes = (int)T::BYTES;
-#define SET_SMEM(KIND)                                                                                         \
-  MCV_CUDA(cudaFuncSetAttribute(stage_kernel<D, S::CX, S::CY, S::NT, KIND>,                                 \
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),                       \
-           "set stage kernel shared memory")
-  SET_SMEM(RK3_S1);
-  SET_SMEM(RK3_S2);
-  SET_SMEM(RK3_S3);
-  SET_SMEM(RK4_S1);
-  SET_SMEM(RK4_S2);
-  SET_SMEM(RK4_S3);
-  SET_SMEM(RK4_S4);
-#undef SET_SMEM
-  return MCV_OK;
-}
-
-template <int D>
-void launch_halo(mcv_handle *h, double *const st[3]) {
+HaloArgs halo_args(mcv_handle *h, int s, int c) {
   HaloArgs a{};
-  a.u = st[0];
-  a.v = st[1];
-  a.phi = st[2];
   a.bnd = h->bnd;
   a.Mtab = h->Mtab;
   a.Ntab = h->Ntab;
@@ -230,76 +288,131 @@ void launch_halo(mcv_handle *h, double *const st[3]) {
   a.dx2 = h->dx2;
   a.dx3 = h->dx3;
   a.members = h->members;
-  const long long threads = 24LL * (h->H + 1) * h->g.n * h->members;
-  const int block = 128;
-  halo_kernel<D><<<(unsigned)((threads + block - 1) / block), block, 0, h->stream>>>(h->g, a);
-}
-
-StageArgs stage_args(mcv_handle *h, double *const in[3], double *const base[3], double *const out[3], double inc) {
-  StageArgs a{};
-  a.us = in[0]; a.vs = in[1]; a.ps = in[2];
-  a.u0 = base[0]; a.v0 = base[1]; a.p0 = base[2];
-  a.uo = out[0]; a.vo = out[1]; a.po = out[2];
-  a.aU = h->acc[0]; a.aV = h->acc[1]; a.aP = h->acc[2];
-  a.sqrtG = h->sqrtG; a.ig11 = h->ig11; a.ig12 = h->ig12; a.ig22 = h->ig22; a.fcor = h->fcor;
-  a.phis = h->phis;
-  a.bnd = h->bnd;
-  a.inc = inc;
+  const int kind = stage_kind(h, s);
+  if (!h->mixed) {
+    double *const *out = (kind == RK3_S1 || kind == RK4_S1 || kind == RK4_S3) ? h->A
+                         : (kind == RK3_S2 || kind == RK4_S2)                  ? h->B
+                                                                               : h->Y;
+    a.u = out[0]; a.v = out[1]; a.phi = out[2];
+    return a;
+  }
+  if (last_stage(kind)) {
+    a.u = h->S[1 - c][0]; a.v = h->S[1 - c][1]; a.phi = h->S[1 - c][2];
+    return a;
+  }
+  a.u = h->S[c][0]; a.v = h->S[c][1]; a.phi = h->S[c][2];
+  float *const *d = (kind == RK3_S1 || kind == RK4_S1 || kind == RK4_S3) ? h->DA : h->DB;
+  a.du = d[0]; a.dv = d[1]; a.dp = d[2];
+  a.bnd32 = h->bnd32;
   return a;
 }
 
-// Stage s of one RK step on every member (the stage sequence of RK3_TVD /
-// RK4, src/time_scheme_mod.F90:13-69): the fused stage kernel, then the halo
-// kernel on the stage's output.
-template <int D>
-void enqueue_stage(mcv_handle *h, int s, cudaEvent_t mid = nullptr) {
-  const double dt = h->dt;
-  double *const *out = nullptr;
-  if (h->scheme == MCV_RK3_TVD) {
-    switch (s) {
-      case 0: launch_stage<D, RK3_S1>(h, stage_args(h, h->Y, h->Y, h->A, dt)); out = h->A; break;
-      case 1: launch_stage<D, RK3_S2>(h, stage_args(h, h->A, h->Y, h->B, 0.25 * dt)); out = h->B; break;
-      default: launch_stage<D, RK3_S3>(h, stage_args(h, h->B, h->Y, h->Y, 2. / 3. * dt)); out = h->Y; break;
-    }
+void launch_halo(mcv_handle *h, int s, int c) {
+  const HaloArgs a = halo_args(h, s, c);
+  const bool mixed_inc = h->mixed && !last_stage(stage_kind(h, s));
+  const long long threads = 24LL * (h->H + 1) * h->g.n * h->members;
+  const int block = 128;
+  const unsigned grid = (unsigned)((threads + block - 1) / block);
+  if (h->order == 3) {
+    if (mixed_inc) halo_kernel<3, true><<<grid, block, 0, h->stream>>>(h->g, a);
+    else halo_kernel<3, false><<<grid, block, 0, h->stream>>>(h->g, a);
   } else {
-    switch (s) {
-      case 0: launch_stage<D, RK4_S1>(h, stage_args(h, h->Y, h->Y, h->A, 0.5 * dt)); out = h->A; break;
-      case 1: launch_stage<D, RK4_S2>(h, stage_args(h, h->A, h->Y, h->B, 0.5 * dt)); out = h->B; break;
-      case 2: launch_stage<D, RK4_S3>(h, stage_args(h, h->B, h->Y, h->A, dt)); out = h->A; break;
-      default: launch_stage<D, RK4_S4>(h, stage_args(h, h->A, h->Y, h->Y, dt)); out = h->Y; break;
+    if (mixed_inc) halo_kernel<4, true><<<grid, block, 0, h->stream>>>(h->g, a);
+    else halo_kernel<4, false><<<grid, block, 0, h->stream>>>(h->g, a);
+  }
+}
+
+void launch_stage(mcv_handle *h, const StageLauncher &L, int s, int c) {
+  GridDesc g = h->g;
+  g.tiles_x = (h->nc + L.CX - 1) / L.CX;
+  g.tiles_y = (h->nc + L.CY - 1) / L.CY;
+  L.launch[stage_kind(h, s)](dim3(g.tiles_x * g.tiles_y, 6, h->members), h->stream, g, stage_args(h, s, c));
+}
+
+// Stage s of one RK step on every member: fused stage kernel, then the halo
+// kernel on the stage's output.
+void enqueue_stage(mcv_handle *h, int s, int c, cudaEvent_t mid = nullptr) {
+  launch_stage(h, h->cands[h->choice], s, c);
+  if (mid) cudaEventRecord(mid, h->stream);
+  launch_halo(h, s, c);
+}
+
+// Time every candidate tile shape on this grid with the second stage kind,
+// which does not modify its own inputs, and keep the fastest.
+int autotune(mcv_handle *h) {
+  if (h->choice >= 0) return MCV_OK;
+  h->tune_ms.assign(h->ncands, -1.f);
+  cudaEvent_t e0, e1;
+  MCV_CUDA(cudaEventCreate(&e0), "event");
+  MCV_CUDA(cudaEventCreate(&e1), "event");
+  float best = 1e30f;
+  int besti = 0;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < h->ncands && e == cudaSuccess; ++i) {
+    const StageLauncher &L = h->cands[i];
+    launch_stage(h, L, 1, h->cur);  // warm-up
+    cudaEventRecord(e0, h->stream);
+    for (int r = 0; r < 3; ++r) launch_stage(h, L, 1, h->cur);
+    cudaEventRecord(e1, h->stream);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    h->tune_ms[i] = ms / 3.f;
+    if (e == cudaSuccess && h->tune_ms[i] < best) {
+      best = h->tune_ms[i];
+      besti = i;
     }
   }
-  if (mid) cudaEventRecord(mid, h->stream);
-  launch_halo<D>(h, out);
-}
-
-int num_stages(const mcv_handle *h) { return h->scheme == MCV_RK3_TVD ? 3 : 4; }
-
-void enqueue_stage_any(mcv_handle *h, int s, cudaEvent_t mid = nullptr) {
-  if (h->order == 3) enqueue_stage<3>(h, s, mid);
-  else enqueue_stage<4>(h, s, mid);
-}
-
-void enqueue_step(mcv_handle *h) {
-  for (int s = 0; s < num_stages(h); ++s) enqueue_stage_any(h, s);
-}
-
-int build_graph(mcv_handle *h) {
-  if (h->graph_exec) return MCV_OK;
-  MCV_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin step capture");
-  enqueue_step(h);
-  cudaError_t le = cudaGetLastError();
-  cudaGraph_t graph = nullptr;
-  cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
-  if (le != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    return cuda_fail(le, "launch during step capture");
-  }
-  MCV_CUDA(ce, "end step capture");
-  h->graph = graph;
-  MCV_CUDA(cudaGraphInstantiate(&h->graph_exec, graph, 0), "instantiate step graph");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_fail(e, "autotune stage kernel");
+  h->choice = besti;
   return MCV_OK;
 }
+
+int build_graphs(mcv_handle *h) {
+  if (h->graph_exec[0]) return MCV_OK;
+  if (int rc = autotune(h)) return rc;
+  const int ngraphs = h->mixed ? 2 : 1;
+  for (int c = 0; c < ngraphs; ++c) {
+    MCV_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin step capture");
+    for (int s = 0; s < num_stages(h); ++s) enqueue_stage(h, s, c);
+    cudaError_t le = cudaGetLastError();
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+    if (le != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return cuda_fail(le, "launch during step capture");
+    }
+    MCV_CUDA(ce, "end step capture");
+    cudaError_t ie = cudaGraphInstantiate(&h->graph_exec[c], graph, 0);
+    cudaGraphDestroy(graph);
+    MCV_CUDA(ie, "instantiate step graph");
+  }
+  return MCV_OK;
+}
+
+int ready_to_step(mcv_handle *h) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (!h->geometry_set) return fail(MCV_ERR_ORDER, "mcv_set_geometry must precede stepping");
+  for (int m = 0; m < h->members; ++m)
+    if (!h->member_set[m]) return fail(MCV_ERR_ORDER, "every member must be set before stepping");
+  return build_graphs(h);
+}
+
+// Enqueue nsteps replays of the step graph (split precision alternates the two).
+int enqueue_steps(mcv_handle *h, int nsteps) {
+  for (int s = 0; s < nsteps; ++s) {
+    MCV_CUDA(cudaGraphLaunch(h->graph_exec[h->mixed ? h->cur : 0], h->stream), "launch step graph");
+    if (h->mixed) h->cur = 1 - h->cur;
+  }
+  for (int m = 0; m < h->members; ++m) h->steps_done[m] += nsteps;
+  return MCV_OK;
+}
+
+// The state arrays of the current step.
+double *const *state(mcv_handle *h) { return h->mixed ? h->S[h->cur] : h->Y; }
 
 }  // namespace
 
@@ -307,11 +420,11 @@ extern "C" const char *mcv_last_error(void) { return g_last_error.c_str(); }
 
 extern "C" long long mcv_footprint_bytes(int order, int nc, int scheme, int precision, int members) {
   if ((order != 3 && order != 4) || nc < 2 || members < 1) return -1;
-  (void)precision;
+  if (precision != MCV_FP64 && precision != MCV_MIXED) return -1;
   GridDesc g{};
   int H, npx;
   grid_desc(order, nc, g, H, npx);
-  return (long long)make_layout(g, H, scheme, members).total;
+  return (long long)make_layout(g, H, scheme, precision, members).total;
 }
 
 extern "C" int mcv_create(int order, int nc, int scheme, int precision, double dt, double radius, int members,
@@ -321,8 +434,10 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   if (order != 3 && order != 4) return fail(MCV_ERR_ARG, "order must be 3 (MCV3) or 4 (MCV4)");
   if (nc < 2 || nc > 4096) return fail(MCV_ERR_ARG, "nc out of range [2, 4096]");
   if (scheme != MCV_RK3_TVD && scheme != MCV_RK4) return fail(MCV_ERR_ARG, "scheme must be MCV_RK3_TVD or MCV_RK4");
-  if (precision != MCV_FP64) return fail(MCV_ERR_ARG, "precision not supported by this build");
+  if (precision != MCV_FP64 && precision != MCV_MIXED)
+    return fail(MCV_ERR_ARG, "precision must be MCV_FP64 or MCV_MIXED");
   if (!(dt > 0) || !std::isfinite(dt)) return fail(MCV_ERR_ARG, "dt must be positive and finite");
+  if (!(radius > 0) || !std::isfinite(radius)) return fail(MCV_ERR_ARG, "radius must be positive and finite");
   if (members < 1) return fail(MCV_ERR_ARG, "members must be >= 1");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
@@ -337,6 +452,7 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
 
   mcv_handle *h = new mcv_handle();
   h->order = order; h->nc = nc; h->scheme = scheme; h->precision = precision; h->members = members;
+  h->mixed = precision == MCV_MIXED;
   h->dt = dt; h->radius = radius; h->device = dev;
   grid_desc(order, nc, h->g, h->H, h->npx);
   const double pi = 2.0 * std::asin(1.0);
@@ -346,14 +462,18 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->g.inv_dx2 = 1. / (h->g.dx * h->g.dx);
   h->dx2 = h->g.dx * h->g.dx;
   h->dx3 = std::pow(h->g.dx, 3.);
-  int CX = order == 3 ? TileShape<3>::CX : TileShape<4>::CX, CY = order == 3 ? TileShape<3>::CY : TileShape<4>::CY;
-  h->g.tiles_x = (nc + CX - 1) / CX;
-  h->g.tiles_y = (nc + CY - 1) / CY;
   h->member_set.assign(members, 0);
   h->steps_done.assign(members, 0);
-
+  h->phibar_host.assign(members, 0.);
+  h->cands = stage_launchers(order, h->mixed, &h->ncands);
+  for (int i = 0; i < h->ncands; ++i) {
+    cudaError_t e = h->cands[i].prepare();
+    if (e != cudaSuccess) {
+      delete h;
+      return cuda_fail(e, "set stage kernel shared memory");
+    }
+  }
   int rc = upload_tables();
-  if (!rc) rc = (order == 3) ? prepare_kernels<3>() : prepare_kernels<4>();
   if (rc) {
     delete h;
     return rc;
@@ -363,7 +483,7 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
     delete h;
     return cuda_fail(e, "create stream");
   }
-  Layout L = make_layout(h->g, h->H, scheme, members);
+  const Layout L = make_layout(h->g, h->H, scheme, precision, members);
   e = cudaMalloc(&h->pool, L.total);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -374,23 +494,37 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->pool_bytes = L.total;
   char *base = (char *)h->pool;
   for (int k = 0; k < 3; ++k) {
-    h->Y[k] = (double *)(base + L.off_state[k]);
-    h->A[k] = (double *)(base + L.off_state[3 + k]);
-    h->B[k] = (double *)(base + L.off_state[6 + k]);
-    h->acc[k] = scheme == MCV_RK4 ? (double *)(base + L.off_acc[k]) : nullptr;
+    if (!h->mixed) {
+      h->Y[k] = (double *)(base + L.f64_state[k]);
+      h->A[k] = (double *)(base + L.f64_state[3 + k]);
+      h->B[k] = (double *)(base + L.f64_state[6 + k]);
+      h->acc[k] = scheme == MCV_RK4 ? (double *)(base + L.f64_acc[k]) : nullptr;
+    } else {
+      h->S[0][k] = (double *)(base + L.mix_state[k]);
+      h->S[1][k] = (double *)(base + L.mix_state[3 + k]);
+      h->DA[k] = (float *)(base + L.mix_inc[k]);
+      h->DB[k] = (float *)(base + L.mix_inc[3 + k]);
+      h->facc[k] = scheme == MCV_RK4 ? (float *)(base + L.mix_acc[k]) : nullptr;
+    }
   }
-  h->sqrtG = (double *)(base + L.off_metric[0]);
-  h->ig11 = (double *)(base + L.off_metric[1]);
-  h->ig12 = (double *)(base + L.off_metric[2]);
-  h->ig22 = (double *)(base + L.off_metric[3]);
-  h->fcor = (double *)(base + L.off_metric[4]);
-  h->phis = (double *)(base + L.off_phis);
-  h->bnd = (double4 *)(base + L.off_bnd);
-  h->Mtab = (double4 *)(base + L.off_M);
-  h->Ntab = (double4 *)(base + L.off_N);
-  h->giref = (int *)(base + L.off_iref);
-  h->gcoef = (double2 *)(base + L.off_coef);
-  h->partial = (double4 *)(base + L.off_partial);
+  if (h->mixed) {
+    h->phis32 = (float *)(base + L.phis32);
+    h->bnd32 = (float4 *)(base + L.bnd32);
+    h->met1d = (double4 *)(base + L.met1d);
+    h->phibar = (double *)(base + L.phibar);
+  }
+  h->sqrtG = (double *)(base + L.metric[0]);
+  h->ig11 = (double *)(base + L.metric[1]);
+  h->ig12 = (double *)(base + L.metric[2]);
+  h->ig22 = (double *)(base + L.metric[3]);
+  h->fcor = (double *)(base + L.metric[4]);
+  h->phis = (double *)(base + L.phis);
+  h->bnd = (double4 *)(base + L.bnd);
+  h->Mtab = (double4 *)(base + L.M);
+  h->Ntab = (double4 *)(base + L.N);
+  h->giref = (int *)(base + L.iref);
+  h->gcoef = (double2 *)(base + L.coef);
+  h->partial = (double4 *)(base + L.partial);
   // zero everything once: unused pitch padding and halo corners stay finite
   e = cudaMemsetAsync(h->pool, 0, L.total, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -399,7 +533,6 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
     mcv_destroy(h);
     return r;
   }
-  (void)radius;
   *out = h;
   return MCV_OK;
 }
@@ -407,8 +540,8 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
 extern "C" int mcv_destroy(mcv_handle *h) {
   if (!h) return MCV_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-  if (h->graph) cudaGraphDestroy(h->graph);
+  for (int c = 0; c < 2; ++c)
+    if (h->graph_exec[c]) cudaGraphExecDestroy(h->graph_exec[c]);
   if (h->pool) cudaFree(h->pool);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -425,12 +558,11 @@ extern "C" int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double
   const size_t NP = (size_t)npx * npx * 6;
   std::vector<double> g11(NP), g12(NP), g22(NP);
   for (size_t k = 0; k < NP; ++k) {
+    if (matrixIG[4 * k + 1] != matrixIG[4 * k + 2]) return fail(MCV_ERR_ARG, "matrixIG is not symmetric");
     g11[k] = matrixIG[4 * k + 0];
     g12[k] = matrixIG[4 * k + 2];  // IG(1,2) == IG(2,1) (projection_mod.F90:186)
     g22[k] = matrixIG[4 * k + 3];
   }
-  for (size_t k = 0; k < NP; ++k)
-    if (matrixIG[4 * k + 1] != matrixIG[4 * k + 2]) return fail(MCV_ERR_ARG, "matrixIG is not symmetric");
   // ghost weights: iref in 1..Nc, coef with coef**3. (ghost_mod.f90:222)
   std::vector<double2> coef((size_t)H * n);
   for (int hh = 0; hh < H; ++hh)
@@ -464,16 +596,38 @@ extern "C" int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double
           matmul22(m, matrixG + 4 * out, matrixIA + 4 * out);
           Nt[((size_t)(p * 4 + e) * (H + 1) + d) * n + k] = make_double4(m[0], m[1], m[2], m[3]);
         }
+  std::vector<double4> met;
+  if (h->mixed) {
+    // 1-D metric table of the equiangular panel coordinate x_i = (i-1) dx/(D-1) + x_min
+    // (mesh_mod.F90:135-136); the same table serves y because dx == dy.
+    const double R = h->radius, D2R = (2.0 * std::asin(1.0)) / 180.;
+    const size_t centre = (size_t)(npx / 2) + (size_t)npx * (npx / 2);
+    if (std::fabs(sqrtG[centre] / (R * R) - 1.) > 1e-6)
+      return fail(MCV_ERR_ARG, "radius does not match the geometry's sqrtG (mixed precision recomputes the metric)");
+    met.resize(npx);
+    for (int i = 0; i < npx; ++i) {
+      const double x = (double)(i + (1 - H) - 1) * h->g.dx / (double)(h->order - 1) + (-45. * D2R);
+      const double t = std::tan(x), c = std::cos(x), s = std::sin(x);
+      met[i] = make_double4(t, c * c / (R * R), s * c / R, R / (c * c));
+    }
+  }
   int rc;
-  if ((rc = upload_padded(h, h->sqrtG, sqrtG))) return rc;
-  if ((rc = upload_padded(h, h->ig11, g11.data()))) return rc;
-  if ((rc = upload_padded(h, h->ig12, g12.data()))) return rc;
-  if ((rc = upload_padded(h, h->ig22, g22.data()))) return rc;
-  if ((rc = upload_padded(h, h->fcor, f))) return rc;
-  MCV_CUDA(cudaMemcpyAsync(h->Mtab, Mt.data(), Mt.size() * sizeof(double4), cudaMemcpyHostToDevice, h->stream), "upload Mtab");
-  MCV_CUDA(cudaMemcpyAsync(h->Ntab, Nt.data(), Nt.size() * sizeof(double4), cudaMemcpyHostToDevice, h->stream), "upload Ntab");
-  MCV_CUDA(cudaMemcpyAsync(h->giref, ghost_iref, sizeof(int) * (size_t)H * n, cudaMemcpyHostToDevice, h->stream), "upload iref");
-  MCV_CUDA(cudaMemcpyAsync(h->gcoef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, h->stream), "upload coef");
+  if ((rc = upload_padded(h, h->sqrtG, sqrtG, 8))) return rc;
+  if ((rc = upload_padded(h, h->ig11, g11.data(), 8))) return rc;
+  if ((rc = upload_padded(h, h->ig12, g12.data(), 8))) return rc;
+  if ((rc = upload_padded(h, h->ig22, g22.data(), 8))) return rc;
+  if ((rc = upload_padded(h, h->fcor, f, 8))) return rc;
+  MCV_CUDA(cudaMemcpyAsync(h->Mtab, Mt.data(), Mt.size() * sizeof(double4), cudaMemcpyHostToDevice, h->stream),
+           "upload Mtab");
+  MCV_CUDA(cudaMemcpyAsync(h->Ntab, Nt.data(), Nt.size() * sizeof(double4), cudaMemcpyHostToDevice, h->stream),
+           "upload Ntab");
+  MCV_CUDA(cudaMemcpyAsync(h->giref, ghost_iref, sizeof(int) * (size_t)H * n, cudaMemcpyHostToDevice, h->stream),
+           "upload iref");
+  MCV_CUDA(cudaMemcpyAsync(h->gcoef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, h->stream),
+           "upload coef");
+  if (h->mixed)
+    MCV_CUDA(cudaMemcpyAsync(h->met1d, met.data(), sizeof(double4) * npx, cudaMemcpyHostToDevice, h->stream),
+             "upload metric table");
   MCV_CUDA(cudaStreamSynchronize(h->stream), "geometry upload");
   h->sqrtG_host.assign(sqrtG, sqrtG + NP);
   h->geometry_set = true;
@@ -485,12 +639,34 @@ extern "C" int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const d
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   if (m < 0 || m >= h->members) return fail(MCV_ERR_ARG, "member index out of range");
   if (!phi_s || !u || !v || !phi) return fail(MCV_ERR_ARG, "state array is NULL");
+  if (!h->geometry_set) return fail(MCV_ERR_ORDER, "mcv_set_geometry must precede mcv_set_member");
   const long long off = (long long)m * h->g.mstride;
+  double *const *Y = state(h);
   int rc;
-  if ((rc = upload_padded(h, h->phis + off, phi_s))) return rc;
-  if ((rc = upload_padded(h, h->Y[0] + off, u))) return rc;
-  if ((rc = upload_padded(h, h->Y[1] + off, v))) return rc;
-  if ((rc = upload_padded(h, h->Y[2] + off, phi))) return rc;
+  if ((rc = upload_padded(h, h->phis + off, phi_s, 8))) return rc;
+  if ((rc = upload_padded(h, Y[0] + off, u, 8))) return rc;
+  if ((rc = upload_padded(h, Y[1] + off, v, 8))) return rc;
+  if ((rc = upload_padded(h, Y[2] + off, phi, 8))) return rc;
+  std::vector<float> ps;
+  if (h->mixed) {
+    const int npx = h->npx, H = h->H, n = h->g.n;
+    const size_t NP = (size_t)npx * npx * 6;
+    ps.resize(NP);
+    for (size_t k = 0; k < NP; ++k) ps[k] = (float)phi_s[k];
+    // mean depth: sqrtG-weighted mean of phi over the interior points
+    double num = 0., den = 0.;
+    for (int p = 0; p < 6; ++p)
+      for (int j = H; j < H + n; ++j)
+        for (int i = H; i < H + n; ++i) {
+          const size_t k = (size_t)i + (size_t)npx * ((size_t)j + (size_t)npx * p);
+          num += h->sqrtG_host[k] * phi[k];
+          den += h->sqrtG_host[k];
+        }
+    h->phibar_host[m] = num / den;
+    if ((rc = upload_padded(h, h->phis32 + off, ps.data(), 4))) return rc;
+    MCV_CUDA(cudaMemcpyAsync(h->phibar + m, &h->phibar_host[m], sizeof(double), cudaMemcpyHostToDevice, h->stream),
+             "upload mean depth");
+  }
   MCV_CUDA(cudaStreamSynchronize(h->stream), "member upload");
   h->member_set[m] = 1;
   h->steps_done[m] = 0;
@@ -500,13 +676,8 @@ extern "C" int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const d
 extern "C" int mcv_step_async(mcv_handle *h, int nsteps) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   if (nsteps < 0) return fail(MCV_ERR_ARG, "nsteps must be >= 0");
-  if (!h->geometry_set) return fail(MCV_ERR_ORDER, "mcv_set_geometry must precede mcv_step");
-  for (int m = 0; m < h->members; ++m)
-    if (!h->member_set[m]) return fail(MCV_ERR_ORDER, "every member must be set before mcv_step");
-  if (int rc = build_graph(h)) return rc;
-  for (int s = 0; s < nsteps; ++s) MCV_CUDA(cudaGraphLaunch(h->graph_exec, h->stream), "launch step graph");
-  for (int m = 0; m < h->members; ++m) h->steps_done[m] += nsteps;
-  return MCV_OK;
+  if (int rc = ready_to_step(h)) return rc;
+  return enqueue_steps(h, nsteps);
 }
 
 extern "C" int mcv_sync(mcv_handle *h) {
@@ -531,10 +702,11 @@ extern "C" int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double 
     tmp.resize(NP);
     phi_dst = tmp.data();
   }
+  double *const *Y = state(h);
   int rc;
-  if (u && (rc = download_padded(h, u, h->Y[0] + off))) return rc;
-  if (v && (rc = download_padded(h, v, h->Y[1] + off))) return rc;
-  if (phi_dst && (rc = download_padded(h, phi_dst, h->Y[2] + off))) return rc;
+  if (u && (rc = download_padded(h, u, Y[0] + off))) return rc;
+  if (v && (rc = download_padded(h, v, Y[1] + off))) return rc;
+  if (phi_dst && (rc = download_padded(h, phi_dst, Y[2] + off))) return rc;
   MCV_CUDA(cudaStreamSynchronize(h->stream), "state download");
   if (phi_dst && h->steps_done[m] > 0) {
     // halo corners hold FillValue after correct_bdy_ghost (ghost_mod.f90:161,179)
@@ -557,17 +729,19 @@ extern "C" int mcv_mass_energy(mcv_handle *h, int m, double *mass, double *energ
   if (!h->geometry_set || !h->member_set[m]) return fail(MCV_ERR_ORDER, "geometry and member must be set");
   const long long off = (long long)m * h->g.mstride;
   const double w0 = 1., w1 = (h->order == 3) ? 4. : 3., wden = (h->order == 3) ? 36. : 80.;
+  double *const *Y = state(h);
   if (h->order == 3)
-    mass_energy_kernel<3><<<kPartialBlocks, 256, 0, h->stream>>>(h->g, h->Y[0] + off, h->Y[1] + off, h->Y[2] + off,
-                                                                 h->sqrtG, h->ig11, h->ig12, h->ig22, h->phis + off,
-                                                                 w0, w1, wden, h->partial);
+    mass_energy_kernel<3><<<kPartialBlocks, 256, 0, h->stream>>>(h->g, Y[0] + off, Y[1] + off, Y[2] + off, h->sqrtG,
+                                                                 h->ig11, h->ig12, h->ig22, h->phis + off, w0, w1,
+                                                                 wden, h->partial);
   else
-    mass_energy_kernel<4><<<kPartialBlocks, 256, 0, h->stream>>>(h->g, h->Y[0] + off, h->Y[1] + off, h->Y[2] + off,
-                                                                 h->sqrtG, h->ig11, h->ig12, h->ig22, h->phis + off,
-                                                                 w0, w1, wden, h->partial);
+    mass_energy_kernel<4><<<kPartialBlocks, 256, 0, h->stream>>>(h->g, Y[0] + off, Y[1] + off, Y[2] + off, h->sqrtG,
+                                                                 h->ig11, h->ig12, h->ig22, h->phis + off, w0, w1,
+                                                                 wden, h->partial);
   MCV_CUDA(cudaGetLastError(), "launch mass/energy");
   std::vector<double4> part(kPartialBlocks);
-  MCV_CUDA(cudaMemcpyAsync(part.data(), h->partial, sizeof(double4) * kPartialBlocks, cudaMemcpyDeviceToHost, h->stream),
+  MCV_CUDA(cudaMemcpyAsync(part.data(), h->partial, sizeof(double4) * kPartialBlocks, cudaMemcpyDeviceToHost,
+                           h->stream),
            "download partial sums");
   MCV_CUDA(cudaStreamSynchronize(h->stream), "mass/energy");
   KSum ms{0., 0.}, es{0., 0.};
@@ -588,31 +762,22 @@ extern "C" int mcv_mass_energy(mcv_handle *h, int m, double *mass, double *energ
   return MCV_OK;
 }
 
-static int ready_to_step(mcv_handle *h) {
-  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
-  if (!h->geometry_set) return fail(MCV_ERR_ORDER, "mcv_set_geometry must precede stepping");
-  for (int m = 0; m < h->members; ++m)
-    if (!h->member_set[m]) return fail(MCV_ERR_ORDER, "every member must be set before stepping");
-  return MCV_OK;
-}
-
 extern "C" int mcv_time_steps(mcv_handle *h, int nsteps, double *ms) {
   if (int rc = ready_to_step(h)) return rc;
   if (nsteps < 1 || !ms) return fail(MCV_ERR_ARG, "nsteps >= 1 and ms required");
-  if (int rc = build_graph(h)) return rc;
   cudaEvent_t e0, e1;
   MCV_CUDA(cudaEventCreate(&e0), "event");
   MCV_CUDA(cudaEventCreate(&e1), "event");
   cudaEventRecord(e0, h->stream);
-  for (int s = 0; s < nsteps; ++s) cudaGraphLaunch(h->graph_exec, h->stream);
+  int rc = enqueue_steps(h, nsteps);
   cudaEventRecord(e1, h->stream);
   cudaError_t e = cudaEventSynchronize(e1);
   float t = 0.f;
   if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(e, "timed steps");
-  for (int m = 0; m < h->members; ++m) h->steps_done[m] += nsteps;
   *ms = t;
   return MCV_OK;
 }
@@ -623,13 +788,15 @@ extern "C" int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, dou
   const int S = num_stages(h);
   std::vector<cudaEvent_t> ev((size_t)nsteps * S * 3);
   for (auto &e : ev) MCV_CUDA(cudaEventCreate(&e), "event");
-  for (int it = 0; it < nsteps; ++it)
+  for (int it = 0; it < nsteps; ++it) {
     for (int s = 0; s < S; ++s) {
       cudaEvent_t *e = &ev[((size_t)it * S + s) * 3];
       cudaEventRecord(e[0], h->stream);
-      enqueue_stage_any(h, s, e[1]);
+      enqueue_stage(h, s, h->cur, e[1]);
       cudaEventRecord(e[2], h->stream);
     }
+    if (h->mixed) h->cur = 1 - h->cur;
+  }
   cudaError_t err = cudaGetLastError();
   if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
   double st[4] = {0, 0, 0, 0}, ha = 0;
@@ -647,5 +814,34 @@ extern "C" int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, dou
   for (int s = 0; s < 4; ++s) stage_ms[s] = s < S ? st[s] / nsteps : 0.;
   *halo_ms = ha / ((double)nsteps * S);
   for (int m = 0; m < h->members; ++m) h->steps_done[m] += nsteps;
+  return MCV_OK;
+}
+
+extern "C" int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, float *ms) {
+  if (int rc = ready_to_step(h)) return rc;
+  if (ncand) *ncand = h->ncands;
+  if (chosen) *chosen = h->choice;
+  for (int i = 0; i < h->ncands; ++i) {
+    if (shapes) {
+      shapes[3 * i] = h->cands[i].CX;
+      shapes[3 * i + 1] = h->cands[i].CY;
+      shapes[3 * i + 2] = h->cands[i].NT;
+    }
+    if (ms) ms[i] = h->tune_ms[i];
+  }
+  return MCV_OK;
+}
+
+extern "C" int mcv_select_tile(mcv_handle *h, int index) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (index < -1 || index >= h->ncands) return fail(MCV_ERR_ARG, "tile index out of range");
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int c = 0; c < 2; ++c)
+    if (h->graph_exec[c]) {
+      cudaGraphExecDestroy(h->graph_exec[c]);
+      h->graph_exec[c] = nullptr;
+    }
+  h->choice = index;  // -1: autotune again before the next step
+  if (index >= 0 && (int)h->tune_ms.size() != h->ncands) h->tune_ms.assign(h->ncands, -1.f);
   return MCV_OK;
 }

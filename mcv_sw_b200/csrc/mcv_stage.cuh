@@ -1,0 +1,514 @@
+// mcv_stage.cuh -- sm_100a stage kernel (K1) of one RK stage of MCV_SW.
+//
+//  stage_kernel   (K1): per panel tile, the whole spatial operator
+//                 (src/spatial_operators_mod.F90:12-133) fused with the RK
+//                 stage update (src/time_scheme_mod.F90:71-123, the RK4
+//                 combine :38-42) and phi = phiG/sqrtG.  Contravariant winds,
+//                 phiG, K and E are recomputed from (u, v, phi) in the tile.
+//                 Two arithmetic policies share the kernel: FP64 throughout,
+//                 and split precision (FP32 tendencies on phi - phibar from an
+//                 FP64 state, FP32 stage increments, metric recomputed per
+//                 point in FP64 from 1-D tables).
+//  halo_kernel    (K2): correct_bdy_ghost (src/time_scheme_mod.F90:125-142):
+//                 ghost fill with the FP64 edge interpolation
+//                 (src/ghost_mod.f90:88-227), boundary unification of the 12
+//                 edges and 8 vertices (src/spatial_operators_mod.F90:282-388),
+//                 sphere<->panel wind rotations on the strips (:408-492).
+//
+// Device layout of a padded field: [member][panel][row j][pitch P] with
+// padded indices (reference index - ips), P >= npx rounded up to 16 elements.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+namespace mcv {
+
+// RK stage kinds: which combination of stage input, RK base and tendency
+// makes the stage output.
+enum StageKind : int {
+  RK3_S1 = 0,  // y1 = y0 + dt L(y0)                          time_scheme_mod.F90:60-61
+  RK3_S2 = 1,  // y2 = 3/4 y0 + 1/4 y1 + 1/4 dt L(y1)         :89-105
+  RK3_S3 = 2,  // y  = 1/3 y0 + 2/3 y2 + 2/3 dt L(y2)         :107-123
+  RK4_S1 = 3,  // y2 = y0 + dt/2 k1; acc = k1                  :27-28
+  RK4_S2 = 4,  // y3 = y0 + dt/2 k2; acc += 2 k2               :30-31
+  RK4_S3 = 5,  // y4 = y0 + dt k3;   acc += 2 k3               :33-34
+  RK4_S4 = 6,  // y  = y0 + dt (acc + k4)/6                    :36-42
+};
+__host__ __device__ constexpr bool first_stage(int k) { return k == RK3_S1 || k == RK4_S1; }
+__host__ __device__ constexpr bool last_stage(int k) { return k == RK3_S3 || k == RK4_S4; }
+
+struct GridDesc {
+  int n;      // PVs per panel edge (nPVx)
+  int np;     // padded points per direction
+  int P;      // row pitch in elements
+  int Nc;     // cells per panel edge
+  int tiles_x, tiles_y;
+  long long plane;    // np * P
+  long long mstride;  // 6 * plane
+  double dx;          // cell width in radians
+  double inv_dx, inv_2dx, inv_dx2;  // 1/dx, 1/(2 dx), 1/dx**2
+};
+
+struct StageArgs {
+  // ---- FP64 policy ----
+  const double *us, *vs, *ps;  // stage input u, v, phi (padded, halo valid)
+  const double *u0, *v0, *p0;  // RK base (interior; may alias the outputs)
+  double *uo, *vo, *po;        // stage output (interior written here)
+  double *aU, *aV, *aP;        // RK4 tendency accumulators
+  const double *sqrtG, *ig11, *ig12, *ig22, *fcor;  // metric planes [6][np][P]
+  const double *phis;                               // [M][6][np][P]
+  double4 *bnd;  // raw boundary copy [M][6][4][n] {u, v, phi, 0}
+  double inc;    // dt or dt/2 (update_stat's inc_t) or the RK3 tendency weight
+  // ---- split-precision policy ----
+  const double *yu, *yv, *yp;  // FP64 state Y (RK base and stage-1 input), padded; the last
+                               // stage writes Y + increment to uo/vo/po (the other state buffer)
+  const float *du, *dv, *dp;  // FP32 increment of the stage input over Y (stages >= 2)
+  float *eu, *ev, *ep;        // FP32 increment written by intermediate stages
+  float *fU, *fV, *fP;        // FP32 RK4 accumulators
+  const float *phis32;        // FP32 phi_s [M][6][np][P]
+  const double4 *met1d;       // per padded index: {tan, cos^2/R^2, sin cos/R, R sec^2}
+  const double *phibar;       // mean depth per member
+  float4 *bnd32;              // raw boundary copy of the increment
+  double two_omega;
+  float wd, wt;  // increment = wd * (input increment) + wt * tendency (RK3/RK4 weights)
+};
+
+// ---------------------------------------------------------------------------
+// One-dimensional MCV building blocks (src/spatial_operators_mod.F90:136-246).
+// Divisions by the cell width are multiplications by precomputed reciprocals,
+// one rounding away from the reference's quotient.
+// ---------------------------------------------------------------------------
+template <int D, typename R>
+__device__ __forceinline__ R polyfit_left(const R *pv, R inv) {
+  // inv = 1/dh (MCV3) or 1/(2 dh) (MCV4)
+  if constexpr (D == 3) return -(pv[2] - R(4) * pv[1] + R(3) * pv[0]) * inv;
+  else return (-(R(11) * pv[0]) + R(18) * pv[1] - R(9) * pv[2] + R(2) * pv[3]) * inv;
+}
+template <int D, typename R>
+__device__ __forceinline__ R polyfit_right(const R *pv, R inv) {
+  if constexpr (D == 3) return (pv[0] - R(4) * pv[1] + R(3) * pv[2]) * inv;
+  else return (R(11) * pv[3] - R(18) * pv[2] + R(9) * pv[1] - R(2) * pv[0]) * inv;
+}
+template <typename R>
+__device__ __forceinline__ R riemann(R fL, R fR, R qL, R qR, R lam) {
+  return R(0.5) * ((fL + fR) - lam * (qR - qL));
+}
+
+// Cell-width constants in the arithmetic type of the sweep.
+template <typename R>
+struct Widths {
+  R dx, inv_dx, inv_2dx, inv_dx2;
+  __device__ explicit Widths(const GridDesc &g)
+      : dx(R(g.dx)), inv_dx(R(g.inv_dx)), inv_2dx(R(g.inv_2dx)), inv_dx2(R(g.inv_dx2)) {}
+};
+
+// Derivatives at the D points of the centre cell of a 3-cell window
+// (3D-2 values with stride S): calc_tendP, src/spatial_operators_mod.F90:136-202.
+template <int D, int S, typename R>
+__device__ __forceinline__ void cell_derivs(R out[D], const R *f, const R *q, R lamL, R lamR, const Widths<R> &w) {
+  const R ip = (D == 3) ? w.inv_dx : w.inv_2dx;
+  R c1[D], c2[D], c3[D], d1[D], d2[D], d3[D];
+#pragma unroll
+  for (int m = 0; m < D; ++m) {
+    c1[m] = f[m * S];
+    c2[m] = f[(D - 1 + m) * S];
+    c3[m] = f[(2 * D - 2 + m) * S];
+    d1[m] = q[m * S];
+    d2[m] = q[(D - 1 + m) * S];
+    d3[m] = q[(2 * D - 2 + m) * S];
+  }
+  const R fxL1 = polyfit_right<D>(c1, ip), fxL2 = polyfit_right<D>(c2, ip);
+  const R fxR1 = polyfit_left<D>(c2, ip), fxR2 = polyfit_left<D>(c3, ip);
+  const R qxL1 = polyfit_right<D>(d1, ip), qxL2 = polyfit_right<D>(d2, ip);
+  const R qxR1 = polyfit_left<D>(d2, ip), qxR2 = polyfit_left<D>(d3, ip);
+  out[0] = riemann(fxL1, fxR1, qxL1, qxR1, lamL);
+  out[D - 1] = riemann(fxL2, fxR2, qxL2, qxR2, lamR);
+  if constexpr (D == 3) {
+    const R fxVIA = (c2[2] - c2[0]) * w.inv_dx;
+    out[1] = R(1.5) * fxVIA - R(0.25) * (out[0] + out[2]);
+  } else {
+    const R fxVIA = (c2[3] - c2[0]) * w.inv_dx;
+    const R fxxc = R(4.5) * (c2[0] - c2[1] - c2[2] + c2[3]) * w.inv_dx2;
+    out[1] = R(4. / 3.) * fxVIA - (R(4) * out[0] + R(5) * out[3]) / R(27) - R(4. / 27.) * w.dx * fxxc;
+    out[2] = R(4. / 3.) * fxVIA - (R(5) * out[0] + R(4) * out[3]) / R(27) + R(4. / 27.) * w.dx * fxxc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K1: fused spatial operator + RK stage on one tile of CX x CY cells.
+// ---------------------------------------------------------------------------
+template <int D, int CX, int CY, typename R>
+struct Tile {
+  static constexpr int H = D - 1;
+  static constexpr int TX = CX * (D - 1) + 1;  // tile points per row (max)
+  static constexpr int TY = CY * (D - 1) + 1;
+  static constexpr int LX = TX + 2 * H;        // loaded row length (odd: no bank conflicts on column walks)
+  static constexpr int LY = TY + 2 * H;
+  static constexpr int A = LX * LY;  // loaded rectangle (corners unused)
+  static constexpr int I = TX * TY;  // tile interior
+  // shared-memory carve (elements of R): full-rectangle arrays ...
+  static constexpr int U = 0, V = A, E = 2 * A, PG = 3 * A, PGU = 4 * A, PGV = 5 * A;
+  // ... interior-only arrays ...
+  static constexpr int SG = 6 * A, CU = SG + I, CV = CU + I, FC = CV + I;
+  // ... interface eigenvalues and upwind signs ...
+  static constexpr int LAMX = FC + I;                // [TY][CX+1]
+  static constexpr int SGNX = LAMX + TY * (CX + 1);
+  static constexpr int LAMY = SGNX + TY * (CX + 1);  // [TX][CY+1]
+  static constexpr int SGNY = LAMY + TX * (CY + 1);
+  // ... sweep results [3][TY][TX] each ...
+  static constexpr int XR = SGNY + TX * (CY + 1);
+  static constexpr int YR = XR + 3 * I;
+  static constexpr int TOTAL = YR + 3 * I;
+  // 1-D metric tables (split precision): [LX] and [LY] double4 after the R arrays
+  static constexpr size_t MET_OFF = ((size_t)TOTAL * sizeof(R) + 31) / 32 * 32;
+  static constexpr size_t bytes(bool mixed) {
+    return mixed ? MET_OFF + (size_t)(LX + LY) * sizeof(double4) : (size_t)TOTAL * sizeof(R);
+  }
+  static_assert(LX % 2 == 1, "odd shared row length");
+};
+
+template <int D, int CX, int CY, int NT, int KIND, bool MIXED>
+__global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const StageArgs a) {
+  using R = std::conditional_t<MIXED, float, double>;
+  using T = Tile<D, CX, CY, R>;
+  constexpr int H = T::H, LX = T::LX;
+  extern __shared__ __align__(32) unsigned char smraw[];
+  R *sm = reinterpret_cast<R *>(smraw);
+  const int tile = blockIdx.x, panel = blockIdx.y, mem = blockIdx.z;
+  const int tx = tile % g.tiles_x, ty = tile / g.tiles_x;
+  const int c0x = tx * CX, c0y = ty * CY;
+  const int ncx = min(CX, g.Nc - c0x), ncy = min(CY, g.Nc - c0y);
+  const int X0 = c0x * (D - 1), Y0 = c0y * (D - 1);  // padded coords of the first loaded point
+  const int lxe = ncx * (D - 1) + 1 + 2 * H, lye = ncy * (D - 1) + 1 + 2 * H;
+  const long long pbase = (long long)panel * g.plane;
+  const long long mbase = (long long)mem * g.mstride + pbase;
+  const double4 *metx = reinterpret_cast<const double4 *>(smraw + T::MET_OFF);
+  const double4 *mety = metx + LX;
+
+  if constexpr (MIXED) {
+    // the tile's slices of the 1-D metric table
+    double4 *mx = reinterpret_cast<double4 *>(smraw + T::MET_OFF);
+    for (int k = threadIdx.x; k < LX + T::LY; k += NT) {
+      const int gidx = (k < LX) ? X0 + k : Y0 + (k - LX);
+      if (gidx < g.np) mx[k] = a.met1d[gidx];
+    }
+    __syncthreads();
+  }
+  const double phibar = MIXED ? a.phibar[mem] : 0.;
+
+  // ---- phase 0: load the tile and its halo cross, pointwise quantities ----
+  // (spatial_operators_mod.F90:58-61, eigenvalues :248-280, upwind signs :83-85)
+  {
+    constexpr int PPT = (T::A + NT - 1) / NT;
+    constexpr int NL = MIXED ? 7 : 8;
+    double r[NL][PPT];
+    bool ok[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const int idx = threadIdx.x + k * NT;
+      const int ly = idx / LX, lx = idx - ly * LX;
+      const bool xh = (lx < H) || (lx >= lxe - H);
+      const bool yh = (ly < H) || (ly >= lye - H);
+      ok[k] = idx < T::A && lx < lxe && ly < lye && !(xh && yh);  // tile corners are never read
+      if (ok[k]) {
+        const long long go = (long long)(Y0 + ly) * g.P + (X0 + lx);
+        if constexpr (!MIXED) {
+          r[0][k] = __ldg(a.us + mbase + go);
+          r[1][k] = __ldg(a.vs + mbase + go);
+          r[2][k] = __ldg(a.ps + mbase + go);
+          r[3][k] = __ldg(a.phis + mbase + go);
+          r[4][k] = __ldg(a.sqrtG + pbase + go);
+          r[5][k] = __ldg(a.ig11 + pbase + go);
+          r[6][k] = __ldg(a.ig12 + pbase + go);
+          r[7][k] = __ldg(a.ig22 + pbase + go);
+        } else {
+          r[0][k] = __ldg(a.yu + mbase + go);
+          r[1][k] = __ldg(a.yv + mbase + go);
+          r[2][k] = __ldg(a.yp + mbase + go);
+          r[3][k] = (double)__ldg(a.phis32 + mbase + go);
+          if constexpr (!first_stage(KIND)) {
+            r[4][k] = (double)__ldg(a.du + mbase + go);
+            r[5][k] = (double)__ldg(a.dv + mbase + go);
+            r[6][k] = (double)__ldg(a.dp + mbase + go);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      if (!ok[k]) continue;
+      const int idx = threadIdx.x + k * NT;
+      const int ly = idx / LX, lx = idx - ly * LX;
+      R u, v, phi, dev, phs, sg, g11, g12, g22, pg, fc = R(0);
+      if constexpr (!MIXED) {
+        u = r[0][k]; v = r[1][k]; phi = r[2][k]; dev = phi; phs = r[3][k];
+        sg = r[4][k]; g11 = r[5][k]; g12 = r[6][k]; g22 = r[7][k];
+        pg = phi * sg;
+      } else {
+        double u64 = r[0][k], v64 = r[1][k], p64 = r[2][k];
+        if constexpr (!first_stage(KIND)) {
+          u64 += r[4][k];
+          v64 += r[5][k];
+          p64 += r[6][k];
+        }
+        // equiangular metric from the separable 1-D tables, in FP64
+        // (projection_mod.F90:150-211 with cos^2 y (1 + tan^2 y) = 1)
+        const double4 mx = metx[lx], my = mety[ly];
+        const double rho2 = 1. + mx.x * mx.x + my.x * my.x;
+        const double rinv = rsqrt(rho2);
+        const double sg64 = mx.w * my.w * (rinv * rinv * rinv);
+        u = (R)u64; v = (R)v64; phi = (R)p64; dev = (R)(p64 - phibar); phs = (R)r[3][k];
+        sg = (R)sg64;
+        g11 = (R)(rho2 * mx.y);
+        g22 = (R)(rho2 * my.y);
+        g12 = (R)(rho2 * (mx.z * my.z));
+        pg = (R)(p64 * sg64);
+        // Coriolis f = 2 Omega sin(lat): sin(lat) = tan y / rho on panels 1-4, +-1/rho on 5, 6
+        fc = (R)(a.two_omega * (panel < 4 ? my.x * rinv : (panel == 4 ? rinv : -rinv)));
+      }
+      const R cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
+      const R cv = g12 * u + g22 * v;
+      const R K = R(0.5) * (cu * u + cv * v);
+      sm[T::U + idx] = u;
+      sm[T::V + idx] = v;
+      sm[T::PG + idx] = pg;
+      sm[T::PGU + idx] = pg * cu;
+      sm[T::PGV + idx] = pg * cv;
+      sm[T::E + idx] = dev + phs + K;  // E = phi + phi_s + K (MIXED: phi - phibar; constants drop out of d/dx)
+      const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
+      if (!xh && !yh) {
+        const int ix = lx - H, iy = ly - H;
+        const int ii = iy * T::TX + ix;
+        sm[T::SG + ii] = sg;
+        sm[T::CU + ii] = cu;
+        sm[T::CV + ii] = cv;
+        if constexpr (MIXED) sm[T::FC + ii] = fc;
+        // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
+        if (ix % (D - 1) == 0) {
+          sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
+          sm[T::SGNX + iy * (CX + 1) + ix / (D - 1)] = (cu < R(0)) ? R(-1) : R(1);
+        }
+        if (iy % (D - 1) == 0) {
+          sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
+          sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < R(0)) ? R(-1) : R(1);
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  const int txe = ncx * (D - 1) + 1, tye = ncy * (D - 1) + 1;
+  const Widths<R> w(g);
+
+  // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), item = (row, cell, quantity) ----
+  // quantity 0: flux_x = d(E)/dx, Riemann on u; 1: div_x = d(phiG cU)/dx, Riemann
+  // on phiG; 2: dvdx, upwinded by sign(cU)
+  for (int it = threadIdx.x; it < T::TY * CX * 3; it += NT) {
+    const int r = it % T::TY, rest = it / T::TY;
+    const int c = rest % CX, k = rest / CX;
+    if (r >= tye || c >= ncx) continue;
+    const int w0 = (r + H) * LX + c * (D - 1);
+    const int fo = (k == 0) ? T::E : (k == 1) ? T::PGU : T::V;
+    const int qo = (k == 0) ? T::U : (k == 1) ? T::PG : T::V;
+    const int lo = (k == 2) ? T::SGNX : T::LAMX;
+    R d[D];
+    cell_derivs<D, 1, R>(d, sm + fo + w0, sm + qo + w0, sm[lo + r * (CX + 1) + c], sm[lo + r * (CX + 1) + c + 1], w);
+    R *xr = sm + T::XR + k * T::I + r * T::TX + c * (D - 1);
+    const int mmax = (c == ncx - 1) ? D : D - 1;
+#pragma unroll
+    for (int m = 0; m < D; ++m)
+      if (m < mmax) xr[m] = d[m];
+  }
+
+  // ---- phase Y: y-sweep (:95-125), item = (column, cell, quantity) ----
+  for (int it = threadIdx.x; it < T::TX * CY * 3; it += NT) {
+    const int q = it % T::TX, rest = it / T::TX;
+    const int c = rest % CY, k = rest / CY;
+    if (q >= txe || c >= ncy) continue;
+    const int w0 = (c * (D - 1)) * LX + (q + H);
+    const int fo = (k == 0) ? T::E : (k == 1) ? T::PGV : T::U;
+    const int qo = (k == 0) ? T::V : (k == 1) ? T::PG : T::U;
+    const int lo = (k == 2) ? T::SGNY : T::LAMY;
+    R d[D];
+    cell_derivs<D, LX, R>(d, sm + fo + w0, sm + qo + w0, sm[lo + q * (CY + 1) + c], sm[lo + q * (CY + 1) + c + 1],
+                          w);
+    R *yr = sm + T::YR + k * T::I + (c * (D - 1)) * T::TX + q;
+    const int mmax = (c == ncy - 1) ? D : D - 1;
+#pragma unroll
+    for (int m = 0; m < D; ++m)
+      if (m < mmax) yr[m * T::TX] = d[m];
+  }
+  __syncthreads();
+
+  // ---- phase A: tendency assembly (:127-131), RK stage update, store ----
+  const bool last_x = (c0x + ncx == g.Nc), last_y = (c0y + ncy == g.Nc);
+  const int qown = last_x ? txe : txe - 1;  // seam points belong to the left / lower tile
+  const int rown = last_y ? tye : tye - 1;
+  for (int it = threadIdx.x; it < T::I; it += NT) {
+    const int r = it / T::TX, q = it - r * T::TX;
+    if (q >= qown || r >= rown) continue;
+    const long long go = mbase + (long long)(Y0 + H + r) * g.P + (X0 + H + q);
+    const R sg = sm[T::SG + it], cu = sm[T::CU + it], cv = sm[T::CV + it];
+    const R fc = MIXED ? sm[T::FC + it] : (R)__ldg(a.fcor + pbase + (go - mbase));
+    const R rsg = R(1) / sg;
+    const R flux_x = sm[T::XR + it], div_x = sm[T::XR + T::I + it], dvdx = sm[T::XR + 2 * T::I + it];
+    const R flux_y = sm[T::YR + it], div_y = sm[T::YR + T::I + it], dudy = sm[T::YR + 2 * T::I + it];
+    const R vort = (dvdx - dudy) * rsg;
+    const R tP = -div_x - div_y;
+    const R tU = -flux_x + sg * (vort + fc) * cv;
+    const R tV = -flux_y - sg * (vort + fc) * cu;
+    const int sidx = (r + H) * LX + (q + H);
+    double uo, vo, po;  // values the boundary copy records
+    if constexpr (!MIXED) {
+      const double us = sm[T::U + sidx], vs = sm[T::V + sidx], pgs = sm[T::PG + sidx];
+      double pgo;
+      if constexpr (first_stage(KIND)) {
+        uo = us + a.inc * tU;
+        vo = vs + a.inc * tV;
+        pgo = pgs + a.inc * tP;
+        if constexpr (KIND == RK4_S1) {
+          a.aU[go] = tU;
+          a.aV[go] = tV;
+          a.aP[go] = tP;
+        }
+      } else {
+        const double ub = a.u0[go], vb = a.v0[go], pgb = a.p0[go] * sg;
+        if constexpr (KIND == RK4_S2 || KIND == RK4_S3) {
+          uo = ub + a.inc * tU;
+          vo = vb + a.inc * tV;
+          pgo = pgb + a.inc * tP;
+          a.aU[go] = a.aU[go] + 2. * tU;
+          a.aV[go] = a.aV[go] + 2. * tV;
+          a.aP[go] = a.aP[go] + 2. * tP;
+        } else if constexpr (KIND == RK4_S4) {
+          uo = ub + a.inc * ((a.aU[go] + tU) * (1. / 6.));
+          vo = vb + a.inc * ((a.aV[go] + tV) * (1. / 6.));
+          pgo = pgb + a.inc * ((a.aP[go] + tP) * (1. / 6.));
+        } else if constexpr (KIND == RK3_S2) {
+          uo = 0.75 * ub + 0.25 * us + a.inc * tU;
+          vo = 0.75 * vb + 0.25 * vs + a.inc * tV;
+          pgo = 0.75 * pgb + 0.25 * pgs + a.inc * tP;
+        } else {  // RK3_S3
+          uo = ub * (1. / 3.) + 2. / 3. * us + a.inc * tU;
+          vo = vb * (1. / 3.) + 2. / 3. * vs + a.inc * tV;
+          pgo = pgb * (1. / 3.) + 2. / 3. * pgs + a.inc * tP;
+        }
+      }
+      po = pgo * rsg;  // phi = phiG / sqrtG, time_scheme_mod.F90:81
+      a.uo[go] = uo;
+      a.vo[go] = vo;
+      a.po[go] = po;
+    } else {
+      // tendency of phi = (tendency of phiG) / sqrtG
+      const float tp = tP * rsg;
+      float iu, iv, ip;  // increment over Y
+      if constexpr (KIND == RK4_S4) {
+        iu = a.wt * ((a.fU[go] + tU) * (1.f / 6.f));
+        iv = a.wt * ((a.fV[go] + tV) * (1.f / 6.f));
+        ip = a.wt * ((a.fP[go] + tp) * (1.f / 6.f));
+      } else {
+        iu = a.wt * tU;
+        iv = a.wt * tV;
+        ip = a.wt * tp;
+        if constexpr (KIND == RK3_S2 || KIND == RK3_S3) {
+          iu += a.wd * a.du[go];
+          iv += a.wd * a.dv[go];
+          ip += a.wd * a.dp[go];
+        }
+      }
+      if constexpr (KIND == RK4_S1) {
+        a.fU[go] = tU;
+        a.fV[go] = tV;
+        a.fP[go] = tp;
+      } else if constexpr (KIND == RK4_S2 || KIND == RK4_S3) {
+        a.fU[go] = a.fU[go] + 2.f * tU;
+        a.fV[go] = a.fV[go] + 2.f * tV;
+        a.fP[go] = a.fP[go] + 2.f * tp;
+      }
+      if constexpr (last_stage(KIND)) {
+        // FP64 accumulation of the state into the other state buffer
+        uo = a.yu[go] + (double)iu;
+        vo = a.yv[go] + (double)iv;
+        po = a.yp[go] + (double)ip;
+        a.uo[go] = uo;
+        a.vo[go] = vo;
+        a.po[go] = po;
+      } else {
+        a.eu[go] = iu;
+        a.ev[go] = iv;
+        a.ep[go] = ip;
+        uo = iu;
+        vo = iv;
+        po = ip;
+      }
+    }
+    const int gi = X0 + q, gj = Y0 + r;  // 0-based interior indices
+    const int nn = g.n;
+    if (gi == 0 || gi == nn - 1 || gj == 0 || gj == nn - 1) {
+      // pre-unification boundary values for the halo kernel
+      const long long bo = ((long long)mem * 6 + panel) * 4 * nn;
+      if (!MIXED || last_stage(KIND)) {
+        const double4 val = make_double4(uo, vo, po, 0.);
+        double4 *b = a.bnd + bo;
+        if (gi == 0) b[0 * nn + gj] = val;
+        if (gi == nn - 1) b[1 * nn + gj] = val;
+        if (gj == 0) b[2 * nn + gi] = val;
+        if (gj == nn - 1) b[3 * nn + gi] = val;
+      } else {
+        const float4 val = make_float4((float)uo, (float)vo, (float)po, 0.f);
+        float4 *b = a.bnd32 + bo;
+        if (gi == 0) b[0 * nn + gj] = val;
+        if (gi == nn - 1) b[1 * nn + gj] = val;
+        if (gj == 0) b[2 * nn + gi] = val;
+        if (gj == nn - 1) b[3 * nn + gi] = val;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launch table of one tile shape (used by the tile-shape autotuner).
+// ---------------------------------------------------------------------------
+using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a);
+
+struct StageLauncher {
+  int CX, CY, NT;
+  size_t smem;
+  StageLaunchFn launch[7];  // indexed by StageKind
+  cudaError_t (*prepare)(); // raises the dynamic shared-memory limit of every kind
+};
+
+template <int D, int CX, int CY, int NT, bool MIXED>
+struct StageConfig {
+  using T = Tile<D, CX, CY, std::conditional_t<MIXED, float, double>>;
+  static constexpr size_t SMEM = T::bytes(MIXED);
+  template <int KIND>
+  static void launch(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a) {
+    stage_kernel<D, CX, CY, NT, KIND, MIXED><<<grid, NT, SMEM, s>>>(g, a);
+  }
+  template <int KIND>
+  static cudaError_t attr() {
+    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, KIND, MIXED>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+  }
+  static cudaError_t prepare() {
+    cudaError_t e;
+    if ((e = attr<0>()) || (e = attr<1>()) || (e = attr<2>()) || (e = attr<3>()) || (e = attr<4>()) ||
+        (e = attr<5>()) || (e = attr<6>()))
+      return e;
+    return cudaSuccess;
+  }
+  static StageLauncher make() {
+    static_assert(SMEM <= 227 * 1024, "tile does not fit in shared memory");
+    return StageLauncher{CX, CY, NT, SMEM,
+                         {&launch<0>, &launch<1>, &launch<2>, &launch<3>, &launch<4>, &launch<5>, &launch<6>},
+                         &prepare};
+  }
+};
+
+// Candidate tile shapes per (order, arithmetic), defined in stage_d{3,4}_{f64,mix}.cu.
+const StageLauncher *stage_launchers(int order, bool mixed, int *count);
+
+}  // namespace mcv

@@ -1,0 +1,74 @@
+"""Split precision (FP32 tendencies on phi - phibar, FP64 state accumulation)
+against the FP64 GPU path, which the parity tests tie to the oracle.
+
+Error measure: normalized L2 of the height h = phi/g over cell averages
+(calc_VIA, src/diag_mod.F90:69-93) weighted by the cell areas
+(doc/orderCheck.m:70-75).  Mass drift (M - M0)/M0 with the compensated
+device sums.
+"""
+import numpy as np
+import pytest
+
+from mcv_sw_b200 import api, cases, diag
+from tests.helpers import GRAVITY
+
+pytestmark = pytest.mark.gpu
+
+
+def normalized_l2(geom, a, b):
+    return diag.norms(geom, a, b)[1]
+
+
+def run(geom, st, precision, nsteps):
+    with api.Stepper(st.order, st.nc, st.dt, st.scheme, precision=precision, radius=cases.EARTH_RADIUS) as s:
+        s.set_geometry(geom)
+        s.set_member(0, st.phi_s, st.u, st.v, st.phi)
+        m0, e0 = s.mass_energy(0)
+        s.step(nsteps)
+        m1, e1 = s.mass_energy(0)
+        return s.get_state(0), (m1 - m0) / m0
+
+
+@pytest.mark.parametrize("order,scheme", [(3, "RK4"), (4, "RK3_TVD"), (4, "RK4"), (3, "RK3_TVD")])
+def test_mixed_tracks_fp64(order, scheme):
+    geom = api.Geometry(order, 24, cases.EARTH_RADIUS)
+    st = cases.finish(geom, *cases.balanced_flow(geom, np.random.default_rng(8), 38.6, 0.05, 8, 20.0,
+                                                  mountain=True)[:4], scheme, seconds=6 * 3600.0)
+    ref, _ = run(geom, st, "fp64", st.nsteps)
+    out, drift = run(geom, st, "mixed", st.nsteps)
+    err = normalized_l2(geom, out["phi"] / GRAVITY, ref["phi"] / GRAVITY)
+    assert err < 1e-6, err
+    assert abs(drift) < 1e-10, drift
+    H, n = geom.H, geom.n
+    du = np.abs(out["u"] - ref["u"])[:, H:H + n, H:H + n].max() / np.abs(ref["u"]).max()
+    assert du < 1e-4, du
+
+
+def test_mixed_one_day_error_bound():
+    """MCV4 RK3 at Nc=64 over one simulated day stays within the 1e-5 bound."""
+    geom = api.Geometry(4, 64, cases.EARTH_RADIUS)
+    st = cases.finish(geom, *cases.balanced_flow(geom, np.random.default_rng(9), 38.6, 0.05, 16, 20.0,
+                                                  mountain=True)[:4], "RK3_TVD", seconds=86400.0)
+    ref, _ = run(geom, st, "fp64", st.nsteps)
+    out, drift = run(geom, st, "mixed", st.nsteps)
+    err = normalized_l2(geom, out["phi"] / GRAVITY, ref["phi"] / GRAVITY)
+    assert err < 1e-5, err
+    assert abs(drift) < 1e-9, drift
+
+
+def test_mixed_every_tile_shape_is_bit_identical():
+    geom = api.Geometry(4, 20, cases.EARTH_RADIUS)
+    st = cases.finish(geom, *cases.balanced_flow(geom, np.random.default_rng(5))[:4], "RK3_TVD", nsteps=3)
+    outs = []
+    with api.Stepper(4, 20, st.dt, "RK3_TVD", precision="mixed", radius=cases.EARTH_RADIUS) as s:
+        s.set_geometry(geom)
+        s.set_member(0, st.phi_s, st.u, st.v, st.phi)
+        cands, _ = s.tuning()
+        for i in range(len(cands)):
+            s.select_tile(i)
+            s.set_member(0, st.phi_s, st.u, st.v, st.phi)
+            s.step(3)
+            outs.append(s.get_state(0))
+    for out in outs[1:]:
+        for k in ("u", "v", "phi"):
+            assert np.array_equal(out[k], outs[0][k]), k
