@@ -95,8 +95,12 @@ def balanced_flow(geom, rng, u0=38.6, alpha=0.05, lmax=8, rms=10.0, mountain=Fal
         phi += GRAVITY * harmonic_height(geom, rng, lmin, lmax, rms)
     meta = {"u0": u0, "alpha": alpha, "lmax": lmax, "rms_m": rms}
     if mountain:
+        # summit uniform in longitude and in sin(latitude) within +-20 degrees:
+        # with the ~3000 m mean depth (gh0 = 2.94e4) the balanced flow lowers the
+        # free surface poleward, and a 2000 m summit further poleward would pierce
+        # it (phi -> 0, sqrt(G^ii phi) undefined) in the reference scheme as well
         lon_c = rng.uniform(0.0, 2.0 * np.pi)
-        lat_c = np.arcsin(rng.uniform(-0.8, 0.8))
+        lat_c = float(np.arcsin(rng.uniform(-np.sin(np.radians(20.0)), np.sin(np.radians(20.0)))))
         api.add_mountain(geom, phi, phis, lon_c, lat_c, 2000.0, 1.0e6)
         meta.update(mountain_lon=lon_c, mountain_lat=lat_c)
     return zw, mw, phi, phis, meta
