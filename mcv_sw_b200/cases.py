@@ -1,5 +1,8 @@
 """Seeded synthetic initial states for the benchmark workloads.
 
+The balanced flow's mean geopotential depth is 2.94e4 m^2/s^2 (its equatorial
+value gh0 is set so that the area mean is 2.94e4).
+
 Every state is evaluated at each padded point's own lon/lat, halo included, as
 initTestCase does (src/test_case_mod.F90:13-49), then projected to covariant
 winds with (G IA) (test_case_mod.F90:32-39).  The base flow is the balanced
@@ -88,8 +91,15 @@ def finish(geom, zw, mw, phi, phis, scheme, seconds=None, nsteps=None, cfl=0.5, 
     return InitialState(geom.order, geom.nc, scheme, dt, ns, phis, u, v, phi, zw, mw, meta or {})
 
 
+def equator_gh0(u0, radius=EARTH_RADIUS, mean=GH0):
+    """gh0 of the balanced flow whose area-mean geopotential is `mean`: the flow's
+    phi = gh0 - (R Omega u0 + u0^2/2) sin^2(theta') has area mean
+    gh0 - (R Omega u0 + u0^2/2)/3 for any tilt."""
+    return mean + (radius * 7.292e-5 * u0 + 0.5 * u0 * u0) / 3.0
+
+
 def balanced_flow(geom, rng, u0=38.6, alpha=0.05, lmax=8, rms=10.0, mountain=False, lmin=1):
-    zw, mw, phi = api.tilted_zonal(geom, GH0, u0, alpha)
+    zw, mw, phi = api.tilted_zonal(geom, equator_gh0(u0, geom.radius), u0, alpha)
     phis = np.zeros(geom.shape)
     if lmax:
         phi += GRAVITY * harmonic_height(geom, rng, lmin, lmax, rms)
@@ -132,7 +142,7 @@ def ensemble_member(geom, seed, scheme="RK4", days=2.0):
 def stress(seed=5, nc=1024, order=4, scheme="RK4", nsteps=200, geom=None):
     geom = geom or api.Geometry(order, nc, EARTH_RADIUS)
     rng = np.random.default_rng(seed)
-    zw, mw, phi = api.tilted_zonal(geom, GH0, 38.6, 0.05)
+    zw, mw, phi = api.tilted_zonal(geom, equator_gh0(38.6, geom.radius), 38.6, 0.05)
     phis = np.zeros(geom.shape)
     waves = []
     for R in range(4, 13):

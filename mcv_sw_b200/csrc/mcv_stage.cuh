@@ -104,35 +104,83 @@ struct Widths {
       : dx(R(g.dx)), inv_dx(R(g.inv_dx)), inv_2dx(R(g.inv_2dx)), inv_dx2(R(g.inv_dx2)) {}
 };
 
-// Derivatives at the D points of the centre cell of a 3-cell window
-// (3D-2 values with stride S): calc_tendP, src/spatial_operators_mod.F90:136-202.
-template <int D, int S, typename R>
-__device__ __forceinline__ void cell_derivs(R out[D], const R *f, const R *q, R lamL, R lamR, const Widths<R> &w) {
+// calc_tendP (src/spatial_operators_mod.F90:136-202) applied to every cell of
+// one grid line of `ncells` cells, as the x-sweep (:63-93) and y-sweep (:95-125)
+// do for each row and column.  f and q point to the first point of the halo
+// cell before the line (stride S), lam to the eigenvalue or upwind sign at the
+// line's first interface (stride 1), out to the line's first point (stride OS).
+// Walking the line carries the previous cell's one-sided derivatives, so each
+// interface flux is formed once; it is the value both neighbouring cells'
+// calc_tendP calls produce.  SAME: f and q are the same field (dvdx, dudy).
+template <int D, int NMAX, int S, int OS, bool SAME, typename R>
+__device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, int ncells, R *out,
+                                          const Widths<R> &w) {
   const R ip = (D == 3) ? w.inv_dx : w.inv_2dx;
-  R c1[D], c2[D], c3[D], d1[D], d2[D], d3[D];
+  R cf[D], cq[D];
 #pragma unroll
   for (int m = 0; m < D; ++m) {
-    c1[m] = f[m * S];
-    c2[m] = f[(D - 1 + m) * S];
-    c3[m] = f[(2 * D - 2 + m) * S];
-    d1[m] = q[m * S];
-    d2[m] = q[(D - 1 + m) * S];
-    d3[m] = q[(2 * D - 2 + m) * S];
+    cf[m] = f[m * S];
+    cq[m] = SAME ? cf[m] : q[m * S];
   }
-  const R fxL1 = polyfit_right<D>(c1, ip), fxL2 = polyfit_right<D>(c2, ip);
-  const R fxR1 = polyfit_left<D>(c2, ip), fxR2 = polyfit_left<D>(c3, ip);
-  const R qxL1 = polyfit_right<D>(d1, ip), qxL2 = polyfit_right<D>(d2, ip);
-  const R qxR1 = polyfit_left<D>(d2, ip), qxR2 = polyfit_left<D>(d3, ip);
-  out[0] = riemann(fxL1, fxR1, qxL1, qxR1, lamL);
-  out[D - 1] = riemann(fxL2, fxR2, qxL2, qxR2, lamR);
-  if constexpr (D == 3) {
-    const R fxVIA = (c2[2] - c2[0]) * w.inv_dx;
-    out[1] = R(1.5) * fxVIA - R(0.25) * (out[0] + out[2]);
-  } else {
-    const R fxVIA = (c2[3] - c2[0]) * w.inv_dx;
-    const R fxxc = R(4.5) * (c2[0] - c2[1] - c2[2] + c2[3]) * w.inv_dx2;
-    out[1] = R(4. / 3.) * fxVIA - (R(4) * out[0] + R(5) * out[3]) / R(27) - R(4. / 27.) * w.dx * fxxc;
-    out[2] = R(4. / 3.) * fxVIA - (R(5) * out[0] + R(4) * out[3]) / R(27) + R(4. / 27.) * w.dx * fxxc;
+  // right-end derivatives of the halo cell before the line
+  R fR = polyfit_right<D>(cf, ip), qR = SAME ? fR : polyfit_right<D>(cq, ip);
+  // first cell of the line
+  {
+    R nf[D], nq[D];
+    nf[0] = cf[D - 1];
+    nq[0] = cq[D - 1];
+#pragma unroll
+    for (int m = 1; m < D; ++m) {
+      nf[m] = f[(D - 1 + m) * S];
+      nq[m] = SAME ? nf[m] : q[(D - 1 + m) * S];
+    }
+#pragma unroll
+    for (int m = 0; m < D; ++m) {
+      cf[m] = nf[m];
+      cq[m] = nq[m];
+    }
+  }
+  R fL = polyfit_left<D>(cf, ip), qL = SAME ? fL : polyfit_left<D>(cq, ip);
+  R fluxL = riemann(fR, fL, qR, qL, lam[0]);
+  fR = polyfit_right<D>(cf, ip);
+  qR = SAME ? fR : polyfit_right<D>(cq, ip);
+#pragma unroll
+  for (int c = 0; c < NMAX; ++c) {
+    if (c < ncells) {
+      R nf[D], nq[D];
+      nf[0] = cf[D - 1];
+      nq[0] = cq[D - 1];
+#pragma unroll
+      for (int m = 1; m < D; ++m) {
+        nf[m] = f[((c + 2) * (D - 1) + m) * S];
+        nq[m] = SAME ? nf[m] : q[((c + 2) * (D - 1) + m) * S];
+      }
+      const R nfL = polyfit_left<D>(nf, ip), nqL = SAME ? nfL : polyfit_left<D>(nq, ip);
+      const R fluxR = riemann(fR, nfL, qR, nqL, lam[c + 1]);
+      R o[D];
+      o[0] = fluxL;
+      o[D - 1] = fluxR;
+      if constexpr (D == 3) {
+        const R fxVIA = (cf[2] - cf[0]) * w.inv_dx;
+        o[1] = R(1.5) * fxVIA - R(0.25) * (o[0] + o[2]);
+      } else {
+        const R fxVIA = (cf[3] - cf[0]) * w.inv_dx;
+        const R fxxc = R(4.5) * (cf[0] - cf[1] - cf[2] + cf[3]) * w.inv_dx2;
+        o[1] = R(4. / 3.) * fxVIA - (R(4) * o[0] + R(5) * o[3]) / R(27) - R(4. / 27.) * w.dx * fxxc;
+        o[2] = R(4. / 3.) * fxVIA - (R(5) * o[0] + R(4) * o[3]) / R(27) + R(4. / 27.) * w.dx * fxxc;
+      }
+#pragma unroll
+      for (int m = 0; m < D - 1; ++m) out[(c * (D - 1) + m) * OS] = o[m];
+      if (c == ncells - 1) out[(c * (D - 1) + D - 1) * OS] = o[D - 1];
+#pragma unroll
+      for (int m = 0; m < D; ++m) {
+        cf[m] = nf[m];
+        cq[m] = nq[m];
+      }
+      fR = polyfit_right<D>(cf, ip);
+      qR = SAME ? fR : polyfit_right<D>(cq, ip);
+      fluxL = fluxR;
+    }
   }
 }
 
@@ -200,99 +248,110 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
 
   // ---- phase 0: load the tile and its halo cross, pointwise quantities ----
   // (spatial_operators_mod.F90:58-61, eigenvalues :248-280, upwind signs :83-85)
+  // Per-tile base pointers: every field shares the pitch, so one 32-bit offset
+  // per point addresses all of them.
+  const long long tbase = (long long)Y0 * g.P + X0;
+  const double *t_us = a.us + mbase + tbase, *t_vs = a.vs + mbase + tbase, *t_ps = a.ps + mbase + tbase;
+  const double *t_ph = a.phis + mbase + tbase, *t_sg = a.sqrtG + pbase + tbase;
+  const double *t_11 = a.ig11 + pbase + tbase, *t_12 = a.ig12 + pbase + tbase, *t_22 = a.ig22 + pbase + tbase;
+  const double *t_yu = a.yu + mbase + tbase, *t_yv = a.yv + mbase + tbase, *t_yp = a.yp + mbase + tbase;
+  const float *t_du = a.du + mbase + tbase, *t_dv = a.dv + mbase + tbase, *t_dp = a.dp + mbase + tbase;
+  const float *t_p32 = a.phis32 + mbase + tbase;
   {
-    constexpr int PPT = (T::A + NT - 1) / NT;
+    constexpr int CH = 3;  // points per thread whose loads are in flight together
     constexpr int NL = MIXED ? 7 : 8;
-    double r[NL][PPT];
-    bool ok[PPT];
+    for (int base = 0; base < T::A; base += NT * CH) {
+      double r[NL][CH];
+      bool ok[CH];
 #pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-      const int idx = threadIdx.x + k * NT;
-      const int ly = idx / LX, lx = idx - ly * LX;
-      const bool xh = (lx < H) || (lx >= lxe - H);
-      const bool yh = (ly < H) || (ly >= lye - H);
-      ok[k] = idx < T::A && lx < lxe && ly < lye && !(xh && yh);  // tile corners are never read
-      if (ok[k]) {
-        const long long go = (long long)(Y0 + ly) * g.P + (X0 + lx);
-        if constexpr (!MIXED) {
-          r[0][k] = __ldg(a.us + mbase + go);
-          r[1][k] = __ldg(a.vs + mbase + go);
-          r[2][k] = __ldg(a.ps + mbase + go);
-          r[3][k] = __ldg(a.phis + mbase + go);
-          r[4][k] = __ldg(a.sqrtG + pbase + go);
-          r[5][k] = __ldg(a.ig11 + pbase + go);
-          r[6][k] = __ldg(a.ig12 + pbase + go);
-          r[7][k] = __ldg(a.ig22 + pbase + go);
-        } else {
-          r[0][k] = __ldg(a.yu + mbase + go);
-          r[1][k] = __ldg(a.yv + mbase + go);
-          r[2][k] = __ldg(a.yp + mbase + go);
-          r[3][k] = (double)__ldg(a.phis32 + mbase + go);
-          if constexpr (!first_stage(KIND)) {
-            r[4][k] = (double)__ldg(a.du + mbase + go);
-            r[5][k] = (double)__ldg(a.dv + mbase + go);
-            r[6][k] = (double)__ldg(a.dp + mbase + go);
+      for (int k = 0; k < CH; ++k) {
+        const int idx = base + threadIdx.x + k * NT;
+        const int ly = idx / LX, lx = idx - ly * LX;
+        const bool xh = (lx < H) || (lx >= lxe - H);
+        const bool yh = (ly < H) || (ly >= lye - H);
+        ok[k] = idx < T::A && lx < lxe && ly < lye && !(xh && yh);  // tile corners are never read
+        if (ok[k]) {
+          const int o = ly * g.P + lx;
+          if constexpr (!MIXED) {
+            r[0][k] = __ldg(t_us + o);
+            r[1][k] = __ldg(t_vs + o);
+            r[2][k] = __ldg(t_ps + o);
+            r[3][k] = __ldg(t_ph + o);
+            r[4][k] = __ldg(t_sg + o);
+            r[5][k] = __ldg(t_11 + o);
+            r[6][k] = __ldg(t_12 + o);
+            r[7][k] = __ldg(t_22 + o);
+          } else {
+            r[0][k] = __ldg(t_yu + o);
+            r[1][k] = __ldg(t_yv + o);
+            r[2][k] = __ldg(t_yp + o);
+            r[3][k] = (double)__ldg(t_p32 + o);
+            if constexpr (!first_stage(KIND)) {
+              r[4][k] = (double)__ldg(t_du + o);
+              r[5][k] = (double)__ldg(t_dv + o);
+              r[6][k] = (double)__ldg(t_dp + o);
+            }
           }
         }
       }
-    }
 #pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-      if (!ok[k]) continue;
-      const int idx = threadIdx.x + k * NT;
-      const int ly = idx / LX, lx = idx - ly * LX;
-      R u, v, phi, dev, phs, sg, g11, g12, g22, pg, fc = R(0);
-      if constexpr (!MIXED) {
-        u = r[0][k]; v = r[1][k]; phi = r[2][k]; dev = phi; phs = r[3][k];
-        sg = r[4][k]; g11 = r[5][k]; g12 = r[6][k]; g22 = r[7][k];
-        pg = phi * sg;
-      } else {
-        double u64 = r[0][k], v64 = r[1][k], p64 = r[2][k];
-        if constexpr (!first_stage(KIND)) {
-          u64 += r[4][k];
-          v64 += r[5][k];
-          p64 += r[6][k];
+      for (int k = 0; k < CH; ++k) {
+        if (!ok[k]) continue;
+        const int idx = base + threadIdx.x + k * NT;
+        const int ly = idx / LX, lx = idx - ly * LX;
+        R u, v, phi, dev, phs, sg, g11, g12, g22, pg, fc = R(0);
+        if constexpr (!MIXED) {
+          u = r[0][k]; v = r[1][k]; phi = r[2][k]; dev = phi; phs = r[3][k];
+          sg = r[4][k]; g11 = r[5][k]; g12 = r[6][k]; g22 = r[7][k];
+          pg = phi * sg;
+        } else {
+          double u64 = r[0][k], v64 = r[1][k], p64 = r[2][k];
+          if constexpr (!first_stage(KIND)) {
+            u64 += r[4][k];
+            v64 += r[5][k];
+            p64 += r[6][k];
+          }
+          // equiangular metric from the separable 1-D tables, in FP64
+          // (projection_mod.F90:150-211 with cos^2 y (1 + tan^2 y) = 1)
+          const double4 mx = metx[lx], my = mety[ly];
+          const double rho2 = 1. + mx.x * mx.x + my.x * my.x;
+          const double rinv = rsqrt(rho2);
+          const double sg64 = mx.w * my.w * (rinv * rinv * rinv);
+          u = (R)u64; v = (R)v64; phi = (R)p64; dev = (R)(p64 - phibar); phs = (R)r[3][k];
+          sg = (R)sg64;
+          g11 = (R)(rho2 * mx.y);
+          g22 = (R)(rho2 * my.y);
+          g12 = (R)(rho2 * (mx.z * my.z));
+          pg = (R)(p64 * sg64);
+          // Coriolis f = 2 Omega sin(lat): sin(lat) = tan y / rho on panels 1-4, +-1/rho on 5, 6
+          fc = (R)(a.two_omega * (panel < 4 ? my.x * rinv : (panel == 4 ? rinv : -rinv)));
         }
-        // equiangular metric from the separable 1-D tables, in FP64
-        // (projection_mod.F90:150-211 with cos^2 y (1 + tan^2 y) = 1)
-        const double4 mx = metx[lx], my = mety[ly];
-        const double rho2 = 1. + mx.x * mx.x + my.x * my.x;
-        const double rinv = rsqrt(rho2);
-        const double sg64 = mx.w * my.w * (rinv * rinv * rinv);
-        u = (R)u64; v = (R)v64; phi = (R)p64; dev = (R)(p64 - phibar); phs = (R)r[3][k];
-        sg = (R)sg64;
-        g11 = (R)(rho2 * mx.y);
-        g22 = (R)(rho2 * my.y);
-        g12 = (R)(rho2 * (mx.z * my.z));
-        pg = (R)(p64 * sg64);
-        // Coriolis f = 2 Omega sin(lat): sin(lat) = tan y / rho on panels 1-4, +-1/rho on 5, 6
-        fc = (R)(a.two_omega * (panel < 4 ? my.x * rinv : (panel == 4 ? rinv : -rinv)));
-      }
-      const R cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
-      const R cv = g12 * u + g22 * v;
-      const R K = R(0.5) * (cu * u + cv * v);
-      sm[T::U + idx] = u;
-      sm[T::V + idx] = v;
-      sm[T::PG + idx] = pg;
-      sm[T::PGU + idx] = pg * cu;
-      sm[T::PGV + idx] = pg * cv;
-      sm[T::E + idx] = dev + phs + K;  // E = phi + phi_s + K (MIXED: phi - phibar; constants drop out of d/dx)
-      const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
-      if (!xh && !yh) {
-        const int ix = lx - H, iy = ly - H;
-        const int ii = iy * T::TX + ix;
-        sm[T::SG + ii] = sg;
-        sm[T::CU + ii] = cu;
-        sm[T::CV + ii] = cv;
-        if constexpr (MIXED) sm[T::FC + ii] = fc;
-        // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
-        if (ix % (D - 1) == 0) {
-          sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
-          sm[T::SGNX + iy * (CX + 1) + ix / (D - 1)] = (cu < R(0)) ? R(-1) : R(1);
-        }
-        if (iy % (D - 1) == 0) {
-          sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
-          sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < R(0)) ? R(-1) : R(1);
+        const R cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
+        const R cv = g12 * u + g22 * v;
+        const R K = R(0.5) * (cu * u + cv * v);
+        sm[T::U + idx] = u;
+        sm[T::V + idx] = v;
+        sm[T::PG + idx] = pg;
+        sm[T::PGU + idx] = pg * cu;
+        sm[T::PGV + idx] = pg * cv;
+        sm[T::E + idx] = dev + phs + K;  // E = phi + phi_s + K (MIXED: phi - phibar; constants drop out of d/dx)
+        const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
+        if (!xh && !yh) {
+          const int ix = lx - H, iy = ly - H;
+          const int ii = iy * T::TX + ix;
+          sm[T::SG + ii] = sg;
+          sm[T::CU + ii] = cu;
+          sm[T::CV + ii] = cv;
+          if constexpr (MIXED) sm[T::FC + ii] = fc;
+          // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
+          if (ix % (D - 1) == 0) {
+            sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
+            sm[T::SGNX + iy * (CX + 1) + ix / (D - 1)] = (cu < R(0)) ? R(-1) : R(1);
+          }
+          if (iy % (D - 1) == 0) {
+            sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
+            sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < R(0)) ? R(-1) : R(1);
+          }
         }
       }
     }
@@ -302,43 +361,35 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
   const int txe = ncx * (D - 1) + 1, tye = ncy * (D - 1) + 1;
   const Widths<R> w(g);
 
-  // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), item = (row, cell, quantity) ----
-  // quantity 0: flux_x = d(E)/dx, Riemann on u; 1: div_x = d(phiG cU)/dx, Riemann
-  // on phiG; 2: dvdx, upwinded by sign(cU)
-  for (int it = threadIdx.x; it < T::TY * CX * 3; it += NT) {
-    const int r = it % T::TY, rest = it / T::TY;
-    const int c = rest % CX, k = rest / CX;
-    if (r >= tye || c >= ncx) continue;
-    const int w0 = (r + H) * LX + c * (D - 1);
-    const int fo = (k == 0) ? T::E : (k == 1) ? T::PGU : T::V;
-    const int qo = (k == 0) ? T::U : (k == 1) ? T::PG : T::V;
-    const int lo = (k == 2) ? T::SGNX : T::LAMX;
-    R d[D];
-    cell_derivs<D, 1, R>(d, sm + fo + w0, sm + qo + w0, sm[lo + r * (CX + 1) + c], sm[lo + r * (CX + 1) + c + 1], w);
-    R *xr = sm + T::XR + k * T::I + r * T::TX + c * (D - 1);
-    const int mmax = (c == ncx - 1) ? D : D - 1;
-#pragma unroll
-    for (int m = 0; m < D; ++m)
-      if (m < mmax) xr[m] = d[m];
-  }
-
-  // ---- phase Y: y-sweep (:95-125), item = (column, cell, quantity) ----
-  for (int it = threadIdx.x; it < T::TX * CY * 3; it += NT) {
-    const int q = it % T::TX, rest = it / T::TX;
-    const int c = rest % CY, k = rest / CY;
-    if (q >= txe || c >= ncy) continue;
-    const int w0 = (c * (D - 1)) * LX + (q + H);
-    const int fo = (k == 0) ? T::E : (k == 1) ? T::PGV : T::U;
-    const int qo = (k == 0) ? T::V : (k == 1) ? T::PG : T::U;
-    const int lo = (k == 2) ? T::SGNY : T::LAMY;
-    R d[D];
-    cell_derivs<D, LX, R>(d, sm + fo + w0, sm + qo + w0, sm[lo + q * (CY + 1) + c], sm[lo + q * (CY + 1) + c + 1],
-                          w);
-    R *yr = sm + T::YR + k * T::I + (c * (D - 1)) * T::TX + q;
-    const int mmax = (c == ncy - 1) ? D : D - 1;
-#pragma unroll
-    for (int m = 0; m < D; ++m)
-      if (m < mmax) yr[m * T::TX] = d[m];
+  // ---- phase W: x-walks along rows (spatial_operators_mod.F90:63-93) and
+  // y-walks down columns (:95-125), one item per (line, quantity):
+  // quantity 0: flux = d(E)/dx^i, Riemann on the covariant wind component;
+  // 1: div = d(phiG c^i)/dx^i, Riemann on phiG; 2: dvdx / dudy upwinded by sign(c^i)
+  for (int it = threadIdx.x; it < 3 * (T::TY + T::TX); it += NT) {
+    if (it < 3 * T::TY) {
+      const int r = it % T::TY, k = it / T::TY;
+      if (r >= tye) continue;
+      const R *row = sm + (r + H) * LX;
+      R *xr = sm + T::XR + k * T::I + r * T::TX;
+      if (k == 0)
+        line_walk<D, CX, 1, 1, false, R>(row + T::E, row + T::U, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
+      else if (k == 1)
+        line_walk<D, CX, 1, 1, false, R>(row + T::PGU, row + T::PG, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
+      else
+        line_walk<D, CX, 1, 1, true, R>(row + T::V, row + T::V, sm + T::SGNX + r * (CX + 1), ncx, xr, w);
+    } else {
+      const int j = it - 3 * T::TY;
+      const int q = j % T::TX, k = j / T::TX;
+      if (q >= txe) continue;
+      const R *col = sm + (q + H);
+      R *yr = sm + T::YR + k * T::I + q;
+      if (k == 0)
+        line_walk<D, CY, LX, T::TX, false, R>(col + T::E, col + T::V, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
+      else if (k == 1)
+        line_walk<D, CY, LX, T::TX, false, R>(col + T::PGV, col + T::PG, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
+      else
+        line_walk<D, CY, LX, T::TX, true, R>(col + T::U, col + T::U, sm + T::SGNY + q * (CY + 1), ncy, yr, w);
+    }
   }
   __syncthreads();
 
@@ -349,9 +400,9 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
   for (int it = threadIdx.x; it < T::I; it += NT) {
     const int r = it / T::TX, q = it - r * T::TX;
     if (q >= qown || r >= rown) continue;
-    const long long go = mbase + (long long)(Y0 + H + r) * g.P + (X0 + H + q);
+    const long long go = mbase + tbase + ((H + r) * g.P + (H + q));
     const R sg = sm[T::SG + it], cu = sm[T::CU + it], cv = sm[T::CV + it];
-    const R fc = MIXED ? sm[T::FC + it] : (R)__ldg(a.fcor + pbase + (go - mbase));
+    const R fc = MIXED ? sm[T::FC + it] : (R)__ldg(a.fcor + pbase + tbase + ((H + r) * g.P + (H + q)));
     const R rsg = R(1) / sg;
     const R flux_x = sm[T::XR + it], div_x = sm[T::XR + T::I + it], dvdx = sm[T::XR + 2 * T::I + it];
     const R flux_y = sm[T::YR + it], div_y = sm[T::YR + T::I + it], dudy = sm[T::YR + 2 * T::I + it];

@@ -6,10 +6,10 @@ namespace mcv {
 
 const StageLauncher *stage_launchers_d3_f64(int *count) {
   static const StageLauncher table[] = {
-    StageConfig<3, 12, 12, 320, false>::make(),
-    StageConfig<3, 8, 8, 224, false>::make(),
-    StageConfig<3, 10, 10, 256, false>::make(),
-    StageConfig<3, 16, 8, 384, false>::make()};
+    StageConfig<3, 12, 12, 160, false>::make(),
+    StageConfig<3, 12, 12, 256, false>::make(),
+    StageConfig<3, 8, 8, 128, false>::make(),
+    StageConfig<3, 16, 8, 160, false>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }

@@ -6,10 +6,10 @@ namespace mcv {
 
 const StageLauncher *stage_launchers_d3_mix(int *count) {
   static const StageLauncher table[] = {
-    StageConfig<3, 12, 12, 320, true>::make(),
-    StageConfig<3, 16, 12, 448, true>::make(),
-    StageConfig<3, 16, 16, 512, true>::make(),
-    StageConfig<3, 8, 8, 224, true>::make()};
+    StageConfig<3, 12, 12, 160, true>::make(),
+    StageConfig<3, 12, 12, 256, true>::make(),
+    StageConfig<3, 16, 16, 224, true>::make(),
+    StageConfig<3, 16, 12, 192, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }

@@ -6,10 +6,10 @@ namespace mcv {
 
 const StageLauncher *stage_launchers_d4_f64(int *count) {
   static const StageLauncher table[] = {
-    StageConfig<4, 8, 8, 320, false>::make(),
+    StageConfig<4, 8, 8, 160, false>::make(),
     StageConfig<4, 8, 8, 256, false>::make(),
-    StageConfig<4, 6, 6, 256, false>::make(),
-    StageConfig<4, 12, 8, 448, false>::make()};
+    StageConfig<4, 6, 6, 128, false>::make(),
+    StageConfig<4, 12, 8, 192, false>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }

@@ -6,10 +6,10 @@ namespace mcv {
 
 const StageLauncher *stage_launchers_d4_mix(int *count) {
   static const StageLauncher table[] = {
-    StageConfig<4, 8, 8, 320, true>::make(),
-    StageConfig<4, 12, 8, 448, true>::make(),
-    StageConfig<4, 12, 12, 640, true>::make(),
-    StageConfig<4, 16, 8, 512, true>::make()};
+    StageConfig<4, 8, 8, 160, true>::make(),
+    StageConfig<4, 8, 8, 256, true>::make(),
+    StageConfig<4, 12, 12, 224, true>::make(),
+    StageConfig<4, 16, 8, 224, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }

@@ -66,6 +66,8 @@ def test_seeded_states_reproducible():
     b, _ = cases.small(seed=7, nc=8, geom=g)
     for k in ("u", "v", "phi", "phi_s"):
         assert np.array_equal(getattr(a, k), getattr(b, k))
-    h = (a.phi - api.tilted_zonal(g, cases.GH0, 38.6, 0.05)[2]) / cases.GRAVITY
+    base = api.tilted_zonal(g, cases.equator_gh0(38.6, g.radius), 38.6, 0.05)[2]
+    h = (a.phi - base) / cases.GRAVITY
+    assert abs(cases.area_mean(g, base) - cases.GH0) < 5.0
     assert abs(cases.area_rms(g, h) - 10.0) < 1e-9
     assert a.nsteps * a.dt == pytest.approx(86400.0)
