@@ -105,9 +105,10 @@ int mcv_time_steps(mcv_handle *h, int nsteps, double *ms);
 int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, double *halo_ms);
 
 /* Stage-kernel tile shapes the autotuner timed on this handle's grid (it runs
- * once, before the first step): ncand candidates, shapes[3*i..] = {cells in x,
- * cells in y, threads}, ms[i] = device time per launch, *chosen = the index in
- * use.  No counterpart in the reference (which has no GPU path). */
+ * once, before the first step): ncand candidates, shapes[4*i..] = {cells in x,
+ * cells in y, threads, sweep style (0 per-cell items, 1 line walks)}, ms[i] =
+ * device time per launch, *chosen = the index in use.  No counterpart in the
+ * reference (which has no GPU path). */
 int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, float *ms);
 
 /* Use candidate `index` of mcv_tuning's list instead of the autotuner's choice

@@ -267,12 +267,12 @@ class Stepper:
         return list(st)[:nst], ha.value
 
     def tuning(self):
-        """Autotuner record: list of ((cells_x, cells_y, threads), ms per launch) and the chosen index."""
+        """Autotuner record: list of ((cells_x, cells_y, threads, walk), ms per launch) and the chosen index."""
         n, ch = ctypes.c_int(), ctypes.c_int()
-        shapes = (ctypes.c_int * 48)()
+        shapes = (ctypes.c_int * 64)()
         ms = (ctypes.c_float * 16)()
         _check(lib().mcv_tuning(self.h, ctypes.byref(n), ctypes.byref(ch), shapes, ms))
-        cands = [((shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]), ms[i]) for i in range(n.value)]
+        cands = [(tuple(shapes[4 * i: 4 * i + 4]), ms[i]) for i in range(n.value)]
         return cands, ch.value
 
     def select_tile(self, index):

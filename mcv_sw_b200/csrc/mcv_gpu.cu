@@ -708,15 +708,21 @@ extern "C" int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double 
   if (v && (rc = download_padded(h, v, Y[1] + off))) return rc;
   if (phi_dst && (rc = download_padded(h, phi_dst, Y[2] + off))) return rc;
   MCV_CUDA(cudaStreamSynchronize(h->stream), "state download");
-  if (phi_dst && h->steps_done[m] > 0) {
-    // halo corners hold FillValue after correct_bdy_ghost (ghost_mod.f90:161,179)
+  if (h->steps_done[m] > 0) {
+    // Halo corners are never computed: phi holds FillValue there after
+    // correct_bdy_ghost (ghost_mod.f90:161,179) and the history output marks
+    // u and v the same way (addFillValue, output_mod.F90:230-248).
     const int npx = h->npx, H = h->H;
-    for (int p = 0; p < 6; ++p)
-      for (int j = 0; j < npx; ++j)
-        for (int i = 0; i < npx; ++i) {
-          const bool xh = i < H || i >= npx - H, yh = j < H || j >= npx - H;
-          if (xh && yh) phi_dst[(size_t)i + (size_t)npx * ((size_t)j + (size_t)npx * p)] = -9999999999999999.;
-        }
+    double *fields[3] = {u, v, phi_dst};
+    for (double *fld : fields) {
+      if (!fld) continue;
+      for (int p = 0; p < 6; ++p)
+        for (int j = 0; j < npx; ++j)
+          for (int i = 0; i < npx; ++i) {
+            const bool xh = i < H || i >= npx - H, yh = j < H || j >= npx - H;
+            if (xh && yh) fld[(size_t)i + (size_t)npx * ((size_t)j + (size_t)npx * p)] = -9999999999999999.;
+          }
+    }
   }
   if (phiG)
     for (size_t k = 0; k < NP; ++k) phiG[k] = phi_dst[k] * h->sqrtG_host[k];
@@ -823,9 +829,10 @@ extern "C" int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, f
   if (chosen) *chosen = h->choice;
   for (int i = 0; i < h->ncands; ++i) {
     if (shapes) {
-      shapes[3 * i] = h->cands[i].CX;
-      shapes[3 * i + 1] = h->cands[i].CY;
-      shapes[3 * i + 2] = h->cands[i].NT;
+      shapes[4 * i] = h->cands[i].CX;
+      shapes[4 * i + 1] = h->cands[i].CY;
+      shapes[4 * i + 2] = h->cands[i].NT;
+      shapes[4 * i + 3] = h->cands[i].walk ? 1 : 0;
     }
     if (ms) ms[i] = h->tune_ms[i];
   }

@@ -104,6 +104,38 @@ struct Widths {
       : dx(R(g.dx)), inv_dx(R(g.inv_dx)), inv_2dx(R(g.inv_2dx)), inv_dx2(R(g.inv_dx2)) {}
 };
 
+// calc_tendP (src/spatial_operators_mod.F90:136-202) for the centre cell of a
+// 3-cell window (3D-2 values with stride S): derivatives at its D points.
+template <int D, int S, typename R>
+__device__ __forceinline__ void cell_derivs(R out[D], const R *f, const R *q, R lamL, R lamR, const Widths<R> &w) {
+  const R ip = (D == 3) ? w.inv_dx : w.inv_2dx;
+  R c1[D], c2[D], c3[D], d1[D], d2[D], d3[D];
+#pragma unroll
+  for (int m = 0; m < D; ++m) {
+    c1[m] = f[m * S];
+    c2[m] = f[(D - 1 + m) * S];
+    c3[m] = f[(2 * D - 2 + m) * S];
+    d1[m] = q[m * S];
+    d2[m] = q[(D - 1 + m) * S];
+    d3[m] = q[(2 * D - 2 + m) * S];
+  }
+  const R fxL1 = polyfit_right<D>(c1, ip), fxL2 = polyfit_right<D>(c2, ip);
+  const R fxR1 = polyfit_left<D>(c2, ip), fxR2 = polyfit_left<D>(c3, ip);
+  const R qxL1 = polyfit_right<D>(d1, ip), qxL2 = polyfit_right<D>(d2, ip);
+  const R qxR1 = polyfit_left<D>(d2, ip), qxR2 = polyfit_left<D>(d3, ip);
+  out[0] = riemann(fxL1, fxR1, qxL1, qxR1, lamL);
+  out[D - 1] = riemann(fxL2, fxR2, qxL2, qxR2, lamR);
+  if constexpr (D == 3) {
+    const R fxVIA = (c2[2] - c2[0]) * w.inv_dx;
+    out[1] = R(1.5) * fxVIA - R(0.25) * (out[0] + out[2]);
+  } else {
+    const R fxVIA = (c2[3] - c2[0]) * w.inv_dx;
+    const R fxxc = R(4.5) * (c2[0] - c2[1] - c2[2] + c2[3]) * w.inv_dx2;
+    out[1] = R(4. / 3.) * fxVIA - (R(4) * out[0] + R(5) * out[3]) * R(1. / 27.) - R(4. / 27.) * w.dx * fxxc;
+    out[2] = R(4. / 3.) * fxVIA - (R(5) * out[0] + R(4) * out[3]) * R(1. / 27.) + R(4. / 27.) * w.dx * fxxc;
+  }
+}
+
 // calc_tendP (src/spatial_operators_mod.F90:136-202) applied to every cell of
 // one grid line of `ncells` cells, as the x-sweep (:63-93) and y-sweep (:95-125)
 // do for each row and column.  f and q point to the first point of the halo
@@ -166,8 +198,8 @@ __device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, 
       } else {
         const R fxVIA = (cf[3] - cf[0]) * w.inv_dx;
         const R fxxc = R(4.5) * (cf[0] - cf[1] - cf[2] + cf[3]) * w.inv_dx2;
-        o[1] = R(4. / 3.) * fxVIA - (R(4) * o[0] + R(5) * o[3]) / R(27) - R(4. / 27.) * w.dx * fxxc;
-        o[2] = R(4. / 3.) * fxVIA - (R(5) * o[0] + R(4) * o[3]) / R(27) + R(4. / 27.) * w.dx * fxxc;
+        o[1] = R(4. / 3.) * fxVIA - (R(4) * o[0] + R(5) * o[3]) * R(1. / 27.) - R(4. / 27.) * w.dx * fxxc;
+        o[2] = R(4. / 3.) * fxVIA - (R(5) * o[0] + R(4) * o[3]) * R(1. / 27.) + R(4. / 27.) * w.dx * fxxc;
       }
 #pragma unroll
       for (int m = 0; m < D - 1; ++m) out[(c * (D - 1) + m) * OS] = o[m];
@@ -217,7 +249,7 @@ struct Tile {
   static_assert(LX % 2 == 1, "odd shared row length");
 };
 
-template <int D, int CX, int CY, int NT, int KIND, bool MIXED>
+template <int D, int CX, int CY, int NT, int KIND, bool MIXED, bool WALK>
 __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const StageArgs a) {
   using R = std::conditional_t<MIXED, float, double>;
   using T = Tile<D, CX, CY, R>;
@@ -361,37 +393,79 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
   const int txe = ncx * (D - 1) + 1, tye = ncy * (D - 1) + 1;
   const Widths<R> w(g);
 
-  // ---- phase W: x-walks along rows (spatial_operators_mod.F90:63-93) and
-  // y-walks down columns (:95-125), one item per (line, quantity):
-  // quantity 0: flux = d(E)/dx^i, Riemann on the covariant wind component;
-  // 1: div = d(phiG c^i)/dx^i, Riemann on phiG; 2: dvdx / dudy upwinded by sign(c^i)
-  for (int it = threadIdx.x; it < 3 * (T::TY + T::TX); it += NT) {
-    if (it < 3 * T::TY) {
-      const int r = it % T::TY, k = it / T::TY;
-      if (r >= tye) continue;
-      const R *row = sm + (r + H) * LX;
-      R *xr = sm + T::XR + k * T::I + r * T::TX;
-      if (k == 0)
-        line_walk<D, CX, 1, 1, false, R>(row + T::E, row + T::U, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
-      else if (k == 1)
-        line_walk<D, CX, 1, 1, false, R>(row + T::PGU, row + T::PG, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
-      else
-        line_walk<D, CX, 1, 1, true, R>(row + T::V, row + T::V, sm + T::SGNX + r * (CX + 1), ncx, xr, w);
-    } else {
-      const int j = it - 3 * T::TY;
-      const int q = j % T::TX, k = j / T::TX;
-      if (q >= txe) continue;
-      const R *col = sm + (q + H);
-      R *yr = sm + T::YR + k * T::I + q;
-      if (k == 0)
-        line_walk<D, CY, LX, T::TX, false, R>(col + T::E, col + T::V, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
-      else if (k == 1)
-        line_walk<D, CY, LX, T::TX, false, R>(col + T::PGV, col + T::PG, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
-      else
-        line_walk<D, CY, LX, T::TX, true, R>(col + T::U, col + T::U, sm + T::SGNY + q * (CY + 1), ncy, yr, w);
+  if constexpr (!WALK) {
+    // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), item = (row, cell, quantity) ----
+    // quantity 0: flux_x = d(E)/dx, Riemann on u; 1: div_x = d(phiG cU)/dx, Riemann
+    // on phiG; 2: dvdx, upwinded by sign(cU)
+    for (int it = threadIdx.x; it < T::TY * CX * 3; it += NT) {
+      const int r = it % T::TY, rest = it / T::TY;
+      const int c = rest % CX, k = rest / CX;
+      if (r >= tye || c >= ncx) continue;
+      const int w0 = (r + H) * LX + c * (D - 1);
+      const int fo = (k == 0) ? T::E : (k == 1) ? T::PGU : T::V;
+      const int qo = (k == 0) ? T::U : (k == 1) ? T::PG : T::V;
+      const int lo = (k == 2) ? T::SGNX : T::LAMX;
+      R d[D];
+      cell_derivs<D, 1, R>(d, sm + fo + w0, sm + qo + w0, sm[lo + r * (CX + 1) + c], sm[lo + r * (CX + 1) + c + 1],
+                           w);
+      R *xr = sm + T::XR + k * T::I + r * T::TX + c * (D - 1);
+      const int mmax = (c == ncx - 1) ? D : D - 1;
+#pragma unroll
+      for (int m = 0; m < D; ++m)
+        if (m < mmax) xr[m] = d[m];
     }
+    // ---- phase Y: y-sweep (:95-125), item = (column, cell, quantity) ----
+    for (int it = threadIdx.x; it < T::TX * CY * 3; it += NT) {
+      const int q = it % T::TX, rest = it / T::TX;
+      const int c = rest % CY, k = rest / CY;
+      if (q >= txe || c >= ncy) continue;
+      const int w0 = (c * (D - 1)) * LX + (q + H);
+      const int fo = (k == 0) ? T::E : (k == 1) ? T::PGV : T::U;
+      const int qo = (k == 0) ? T::V : (k == 1) ? T::PG : T::U;
+      const int lo = (k == 2) ? T::SGNY : T::LAMY;
+      R d[D];
+      cell_derivs<D, LX, R>(d, sm + fo + w0, sm + qo + w0, sm[lo + q * (CY + 1) + c],
+                            sm[lo + q * (CY + 1) + c + 1], w);
+      R *yr = sm + T::YR + k * T::I + (c * (D - 1)) * T::TX + q;
+      const int mmax = (c == ncy - 1) ? D : D - 1;
+#pragma unroll
+      for (int m = 0; m < D; ++m)
+        if (m < mmax) yr[m * T::TX] = d[m];
+    }
+    __syncthreads();
+  } else {
+    // ---- phase W: x-walks along rows (spatial_operators_mod.F90:63-93) and
+    // y-walks down columns (:95-125), one item per (line, quantity):
+    // quantity 0: flux = d(E)/dx^i, Riemann on the covariant wind component;
+    // 1: div = d(phiG c^i)/dx^i, Riemann on phiG; 2: dvdx / dudy upwinded by sign(c^i)
+    for (int it = threadIdx.x; it < 3 * (T::TY + T::TX); it += NT) {
+      if (it < 3 * T::TY) {
+        const int r = it % T::TY, k = it / T::TY;
+        if (r >= tye) continue;
+        const R *row = sm + (r + H) * LX;
+        R *xr = sm + T::XR + k * T::I + r * T::TX;
+        if (k == 0)
+          line_walk<D, CX, 1, 1, false, R>(row + T::E, row + T::U, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
+        else if (k == 1)
+          line_walk<D, CX, 1, 1, false, R>(row + T::PGU, row + T::PG, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
+        else
+          line_walk<D, CX, 1, 1, true, R>(row + T::V, row + T::V, sm + T::SGNX + r * (CX + 1), ncx, xr, w);
+      } else {
+        const int j = it - 3 * T::TY;
+        const int q = j % T::TX, k = j / T::TX;
+        if (q >= txe) continue;
+        const R *col = sm + (q + H);
+        R *yr = sm + T::YR + k * T::I + q;
+        if (k == 0)
+          line_walk<D, CY, LX, T::TX, false, R>(col + T::E, col + T::V, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
+        else if (k == 1)
+          line_walk<D, CY, LX, T::TX, false, R>(col + T::PGV, col + T::PG, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
+        else
+          line_walk<D, CY, LX, T::TX, true, R>(col + T::U, col + T::U, sm + T::SGNY + q * (CY + 1), ncy, yr, w);
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   // ---- phase A: tendency assembly (:127-131), RK stage update, store ----
   const bool last_x = (c0x + ncx == g.Nc), last_y = (c0y + ncy == g.Nc);
@@ -526,22 +600,23 @@ using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const GridDesc &g, con
 
 struct StageLauncher {
   int CX, CY, NT;
+  bool walk;  // sweeps as line walks instead of per-cell items
   size_t smem;
   StageLaunchFn launch[7];  // indexed by StageKind
   cudaError_t (*prepare)(); // raises the dynamic shared-memory limit of every kind
 };
 
-template <int D, int CX, int CY, int NT, bool MIXED>
+template <int D, int CX, int CY, int NT, bool MIXED, bool WALK>
 struct StageConfig {
   using T = Tile<D, CX, CY, std::conditional_t<MIXED, float, double>>;
   static constexpr size_t SMEM = T::bytes(MIXED);
   template <int KIND>
   static void launch(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a) {
-    stage_kernel<D, CX, CY, NT, KIND, MIXED><<<grid, NT, SMEM, s>>>(g, a);
+    stage_kernel<D, CX, CY, NT, KIND, MIXED, WALK><<<grid, NT, SMEM, s>>>(g, a);
   }
   template <int KIND>
   static cudaError_t attr() {
-    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, KIND, MIXED>,
+    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, KIND, MIXED, WALK>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
   static cudaError_t prepare() {
@@ -553,7 +628,7 @@ struct StageConfig {
   }
   static StageLauncher make() {
     static_assert(SMEM <= 227 * 1024, "tile does not fit in shared memory");
-    return StageLauncher{CX, CY, NT, SMEM,
+    return StageLauncher{CX, CY, NT, WALK, SMEM,
                          {&launch<0>, &launch<1>, &launch<2>, &launch<3>, &launch<4>, &launch<5>, &launch<6>},
                          &prepare};
   }
