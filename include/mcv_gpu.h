@@ -116,6 +116,26 @@ int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, float *ms);
  * schedule, not the arithmetic: every shape gives bit-identical states. */
 int mcv_select_tile(mcv_handle *h, int index);
 
+/* Total mass and energy of `members` states that already live in the caller's
+ * device memory, without allocating anything.  No counterpart in the reference
+ * (its diagnostics, src/diag_mod.F90:10-67, run on host arrays); this is for
+ * callers that cannot let a library allocate device memory when they ask for
+ * diagnostics: code whose device memory is owned by a framework's caching
+ * allocator, loops that must not pay for cudaMalloc/cudaFree, processes near
+ * their memory budget.
+ * Inputs are device pointers in the reference's layout: u, v, phi, phi_s as
+ * (npx, npx, 6, members) and sqrtG as (npx, npx, 6), column-major, halo
+ * included; matrixIG as (2, 2, npx, npx, 6).  mass, energy are host arrays of
+ * `members`.  stream is a cudaStream_t (NULL: the default stream); the call
+ * waits for its own work.  Limits: members <= 64.  The scratch (one partial sum
+ * per block and member) is a fixed static device array of about 300 KiB held by
+ * every device that loads the library; the first call on a device looks up its
+ * address, so make that first call before any stream capture.  Calls that
+ * overlap on the GPU share the scratch and race. */
+int mcv_mass_energy_noalloc(int order, int nc, int members, const double *u, const double *v, const double *phi,
+                            const double *phi_s, const double *sqrtG, const double *matrixIG, void *stream,
+                            double *mass, double *energy);
+
 /* Release the handle and its device memory. */
 int mcv_destroy(mcv_handle *h);
 

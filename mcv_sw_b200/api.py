@@ -62,6 +62,8 @@ def lib():
         "mcv_profile_step": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
         "mcv_tuning": (ctypes.c_int, [vp, _I, _I, _I, ctypes.POINTER(ctypes.c_float)]),
         "mcv_select_tile": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mcv_mass_energy_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp,
+                                                   vp, _D, _D]),
         "mcv_grid_sizes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _I, _I, _I]),
         "mcv_footprint_bytes": (ctypes.c_longlong, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_int]),
@@ -195,6 +197,17 @@ def sphere_to_cov(geom, zw, mw):
     _check(lib().mcv_sphere_to_cov(geom.npts, _dp(geom.matrixG), _dp(geom.matrixIA), _dp(zw), _dp(mw), _dp(u),
                                    _dp(v)))
     return u, v
+
+
+def mass_energy_noalloc(order, nc, members, u, v, phi, phi_s, sqrtG, matrixIG, stream=0):
+    """mcv_mass_energy_noalloc on caller-owned device memory: the array arguments
+    are device addresses (ints) in the reference's layout.  Returns (mass, energy)
+    as lists of `members` floats."""
+    mass = (ctypes.c_double * members)()
+    energy = (ctypes.c_double * members)()
+    _check(lib().mcv_mass_energy_noalloc(int(order), int(nc), int(members), u, v, phi, phi_s, sqrtG, matrixIG,
+                                         stream or None, mass, energy))
+    return list(mass), list(energy)
 
 
 # ---------------------------------------------------------------- stepping

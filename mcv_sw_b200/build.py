@@ -11,7 +11,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 SOURCES = ["mcv_gpu.cu", "stage_d3_f64.cu", "stage_d3_mix.cu", "stage_d4_f64.cu", "stage_d4_mix.cu",
-           "host_setup.cpp"]
+           "mcv_noalloc.cu", "host_setup.cpp"]
 HEADERS = ["mcv_stage.cuh", "mcv_halo.cuh", "mcv_internal.h", os.path.join("..", "..", "include", "mcv_gpu.h")]
 OBJ_DIR = os.path.join(HERE, "_lib", "obj")
 
