@@ -44,6 +44,9 @@ def parse_args():
     p.add_argument("--error-days", type=float, default=5.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--ensemble", type=int, default=1, help="run the 64-member ensemble block (1 GPU only)")
+    p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving block (0: skip)")
+    p.add_argument("--stress", type=int, default=1, help="run the Nc=1024 roofline-stress block (1 GPU only)")
     return p.parse_args()
 
 
@@ -228,9 +231,90 @@ def time_path(args, st, geom, precision, world, barrier, dist, local):
     cands, chosen = s.tuning()
     out = {"value": value, "ms_per_step": ms / args.steps, "stage_ms": stage_ms, "halo_ms": halo_ms,
            "achieved_gbs": achieved, "bytes_per_pv_step": sum(per_pv), "clocks": clk,
-           "tile": {"chosen_cells_threads": list(cands[chosen][0]),
-                    "candidates": [{"cells_threads": list(c), "ms": round(t, 5)} for c, t in cands]}}
+           "tile": {"shape_fields": ["cells_x", "cells_y", "threads", "line_walks", "ctas_per_sm"],
+                    "chosen": list(cands[chosen][0]),
+                    "candidates": [{"shape": list(c), "ms": round(t, 5)} for c, t in cands]}}
     return s, out
+
+
+def ensemble_block(steps=40, days=2.0, members=64):
+    """Batched ensemble: `members` MCV3 Nc=128 RK4 states (per-member tilt,
+    u0 and harmonic RMS) advanced together, each stage one launch over all
+    members.  Throughput in member-days per second; per-member normalized L2
+    height error of split precision against the FP64 path after `days`."""
+    from mcv_sw_b200 import api, cases, diag
+    geom = api.Geometry(3, 128, cases.EARTH_RADIUS)
+    sts = [cases.ensemble_member(geom, 1000 + m, days=days) for m in range(members)]
+    dt = min(st.dt for st in sts)  # one dt for the batch: CFL 0.5 for every member
+    nsteps = int(np.ceil(days * 86400.0 / dt))
+    dt = days * 86400.0 / nsteps
+    out = {"config": f"{members} members, MCV3 Nc=128 RK4, dt {dt:.2f} s, {days} days ({nsteps} steps)"}
+    finals = {}
+    for precision in ("fp64", "mixed"):
+        with api.Stepper(3, 128, dt, "RK4", members=members, precision=precision, radius=cases.EARTH_RADIUS) as s:
+            s.set_geometry(geom)
+            for m, st in enumerate(sts):
+                s.set_member(m, st.phi_s, st.u, st.v, st.phi)
+            m0 = [s.mass_energy(m)[0] for m in range(members)]
+            s.time_steps(3)
+            ms = s.time_steps(steps)
+            cands, chosen = s.tuning()
+            s.step(nsteps - 3 - steps)
+            finals[precision] = [s.get_state(m)["phi"] / cases.GRAVITY for m in range(members)]
+            drift = [abs(s.mass_energy(m)[0] - m0[m]) / m0[m] for m in range(members)]
+        out[precision] = {"member_days_per_s": members * steps * dt / 86400.0 / (ms / 1e3),
+                          "ms_per_step": ms / steps, "tile_chosen": list(cands[chosen][0]),
+                          "tile_candidates": [{"shape": list(c), "ms": round(t, 5)} for c, t in cands],
+                          "max_abs_mass_drift": max(drift)}
+    errs = [diag.norms(geom, finals["mixed"][m], finals["fp64"][m]) for m in range(members)]
+    l2 = np.array([e[1] for e in errs])
+    out["mixed_height_error_vs_fp64"] = {"L2_median": float(np.median(l2)), "L2_max": float(l2.max()),
+                                         "L1_max": float(max(e[0] for e in errs)),
+                                         "Linf_max": float(max(e[2] for e in errs)),
+                                         "L2_per_member": [float(x) for x in l2]}
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["member_days_per_s"] / out["fp64"]["member_days_per_s"]
+    return out
+
+
+def serving_block(count):
+    """The serving stream's first `count` requests through the continuous-batching
+    server (split precision) and through the plain FP64 one-request-at-a-time loop."""
+    from mcv_sw_b200 import serving
+    reqs, geoms = serving.make_requests(count)
+    keys = sorted({r.key for r in reqs})
+    srv = serving.ForecastServer(precision="mixed", geoms=geoms)
+    srv.prepare(keys)
+    res = srv.run(reqs)
+    stats = dict(srv.stats)
+    srv.close()
+    base = serving.run_one_at_a_time(reqs, precision="fp64", geoms=geoms)
+    return {"requests": count, "stream": "Poisson 20 req/s (seed 4), MCV3/MCV4 50/50, Nc 48/96/192/384 "
+                                         "(.4/.3/.2/.1), 6-120 h, half with mountains; RK3_TVD, CFL 0.45",
+            "server_mixed": serving.summarize(res), "server_stats": stats,
+            "one_at_a_time_fp64": serving.summarize(base)}
+
+
+def stress_block(steps=200):
+    """Roofline stress: MCV4 Nc=1024 RK4; per-stage-kernel achieved GB/s and the
+    halo kernel's share of the step, FP64 and split precision."""
+    from mcv_sw_b200 import api
+    st, geom = build_workload("stress")[:2]
+    n_pv = 6 * geom.n * geom.n
+    out = {"config": f"MCV4 Nc=1024 RK4, {n_pv} PVs per field, {steps} steps"}
+    for precision in ("fp64", "mixed"):
+        with api.Stepper(st.order, st.nc, st.dt, st.scheme, precision=precision, radius=6.371e6) as s:
+            s.set_geometry(geom)
+            s.set_member(0, st.phi_s, st.u, st.v, st.phi)
+            s.time_steps(3)
+            ms = s.time_steps(steps)
+            stage_ms, halo_ms = s.profile_step(3)
+            per_pv = stage_bytes(st.scheme, precision)
+            out[precision] = {"ms_per_step": ms / steps,
+                              "stage_gbs": [b * n_pv / (t * 1e-3) / 1e9 for b, t in zip(per_pv, stage_ms)],
+                              "stage_ms": stage_ms, "halo_ms": halo_ms,
+                              "halo_share_of_step": len(stage_ms) * halo_ms / (ms / steps),
+                              "tile_chosen": list(s.tuning()[0][s.tuning()[1]][0])}
+    return out
 
 
 def run_ours(args):
@@ -298,28 +382,61 @@ def run_ours(args):
                   "mcv_get_state (u, v, phi to pinned host); host wall clock around synchronous calls"}
     main.close()
 
-    # accuracy of split precision against the FP64 path over the full forecast
+    # accuracy of split precision against the FP64 path over the full forecast,
+    # as a daily curve, beside an FP64 "twin" whose initial phi differs by 1e-12
+    # (relative, pointwise): the twin shows how far the flow itself amplifies a
+    # perturbation of that size
     accuracy = None
     if rank == 0 and args.error_days > 0:
         nsteps = int(round(args.error_days * 86400.0 / st.dt))
-        finals, drift = {}, {}
-        for precision in ("fp64", "mixed"):
+        twin_phi = st.phi * (1.0 + 1e-12 * np.random.default_rng(0).standard_normal(st.phi.shape))
+        runs = {"fp64": ("fp64", st.phi), "fp64_twin": ("fp64", twin_phi), "mixed": ("mixed", st.phi)}
+        ncheck = max(1, int(round(args.error_days)))
+        curves, drift = {k: [] for k in runs}, {}
+        for name, (precision, phi0) in runs.items():
             with api.Stepper(st.order, st.nc, st.dt, st.scheme, precision=precision, radius=6.371e6) as s:
                 s.set_geometry(geom)
-                s.set_member(0, st.phi_s, st.u, st.v, st.phi)
+                s.set_member(0, st.phi_s, st.u, st.v, phi0)
                 m0, _ = s.mass_energy(0)
-                s.step(nsteps)
+                done = 0
+                for c in range(ncheck):
+                    k = (nsteps * (c + 1)) // ncheck - done
+                    s.step(k)
+                    done += k
+                    curves[name].append(s.get_state(0)["phi"] / 9.80616)
                 m1, _ = s.mass_energy(0)
-                finals[precision] = s.get_state(0)["phi"] / 9.80616
-                drift[precision] = (m1 - m0) / m0
-        l1, l2, linf = diag.norms(geom, finals["mixed"], finals["fp64"])
+                drift[name] = (m1 - m0) / m0
+        H, n = geom.H, geom.n
+
+        def norms(a, b):
+            if not np.isfinite(a[:, H:H + n, H:H + n]).all():
+                return (float("nan"),) * 3
+            return diag.norms(geom, a, b)
+
+        days = [nsteps * (c + 1) // ncheck * st.dt / 86400.0 for c in range(ncheck)]
+        mixed_curve = [norms(curves["mixed"][c], curves["fp64"][c]) for c in range(ncheck)]
+        twin_curve = [norms(curves["fp64_twin"][c], curves["fp64"][c]) for c in range(ncheck)]
+        l1, l2, linf = mixed_curve[-1]
         accuracy = {"sim_days": nsteps * st.dt / 86400.0, "steps": nsteps,
                     "height_error_vs_fp64": {"L1": l1, "L2": l2, "Linf": linf},
-                    "mass_drift": drift, "reference": "FP64 GPU path (oracle-validated by the parity tests)"}
+                    "curve_days": days, "mixed_L2_curve": [c[1] for c in mixed_curve],
+                    "fp64_twin_L2_curve": [c[1] for c in twin_curve],
+                    "mass_drift": {"fp64": drift["fp64"], "mixed": drift["mixed"]},
+                    "reference": "FP64 GPU path (oracle-validated by the parity tests); fp64_twin: the FP64 "
+                                 "path from phi*(1+1e-12*N(0,1))"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(st)
+    # the other configurations (one GPU: the multi-rank run only measures the main workload)
+    extra = {}
+    if rank == 0 and world == 1:
+        if args.ensemble:
+            extra["ensemble"] = ensemble_block()
+        if args.serve_requests > 0:
+            extra["serving"] = serving_block(args.serve_requests)
+        if args.stress:
+            extra["stress"] = stress_block()
     if rank == 0:
         other = "fp64" if args.precision == "mixed" else "mixed"
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -334,7 +451,7 @@ def run_ours(args):
                 "gpu_launches": args.steps * 2 * nst, "clocks": head["clocks"],
                 "paths": {"fp64": paths["fp64"], "mixed": paths["mixed"]},
                 f"speedup_{args.precision}_vs_{other}": head["value"] / paths[other]["value"],
-                "accuracy": accuracy}
+                "accuracy": accuracy, **extra}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -45,6 +45,7 @@ typedef struct mcv_handle mcv_handle;
 #define MCV_ERR_NOMEM (-3)     /* device allocation failed                   */
 #define MCV_ERR_ORDER (-4)     /* call order (e.g. step before geometry)     */
 #define MCV_ERR_NONFINITE (-5) /* a member's state became NaN/Inf            */
+#define MCV_BUSY 1             /* mcv_query: queued work still running (not an error) */
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *mcv_last_error(void);
@@ -81,9 +82,25 @@ int mcv_step(mcv_handle *h, int nsteps);
 
 /* Queue nsteps on the handle's stream and return without waiting. */
 int mcv_step_async(mcv_handle *h, int nsteps);
-/* Wait for queued work; returns MCV_ERR_NONFINITE if checking was on and a
- * member went non-finite. */
+/* Wait for the work queued on the handle's stream. */
 int mcv_sync(mcv_handle *h);
+/* MCV_OK if all work queued on the handle has finished, MCV_BUSY if some is
+ * still running; never waits. */
+int mcv_query(mcv_handle *h);
+
+/* The members mcv_step / mcv_step_async advance: `count` distinct indices in
+ * `members` (default after mcv_create: all of them).  The others keep their
+ * state and step count untouched; with count = 0 a step enqueues nothing.
+ * A request loop uses this to retire finished forecasts and admit new ones
+ * into free member slots of a running handle.  No counterpart in the
+ * reference (one state per run). */
+int mcv_set_active(mcv_handle *h, int count, const int *members);
+
+/* Failure detection (no counterpart in the reference, which writes NaNs to
+ * its history files): waits for queued work, then flags[m] = 1 (host array of
+ * `members`, may be NULL) where member m's interior u, v or phi holds a NaN or
+ * Inf, else 0.  Returns MCV_ERR_NONFINITE if an active member is flagged. */
+int mcv_check_finite(mcv_handle *h, int *flags);
 
 /* Download member m's state over the padded range (any pointer may be NULL).
  * phiG = phi * sqrtG as src/time_scheme_mod.F90:85 stores it. */
@@ -105,15 +122,19 @@ int mcv_time_steps(mcv_handle *h, int nsteps, double *ms);
 int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, double *halo_ms);
 
 /* Stage-kernel tile shapes the autotuner timed on this handle's grid (it runs
- * once, before the first step): ncand candidates, shapes[4*i..] = {cells in x,
- * cells in y, threads, sweep style (0 per-cell items, 1 line walks)}, ms[i] =
+ * once, before the first step): ncand (at most 16) candidates,
+ * shapes[5*i..] = {cells in x, cells in y, threads, sweep style (0 per-cell
+ * items, 1 line walks), CTAs per SM the kernel's registers allow}, ms[i] =
  * device time per launch, *chosen = the index in use.  No counterpart in the
  * reference (which has no GPU path). */
 int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, float *ms);
 
 /* Use candidate `index` of mcv_tuning's list instead of the autotuner's choice
- * (-1 re-runs the autotuner before the next step).  The tile shape changes the
- * schedule, not the arithmetic: every shape gives bit-identical states. */
+ * (-1 re-runs the autotuner before the next step).  A shape is deterministic.
+ * In FP64, shapes differ only in how the compiler contracts a*b+c into FMA
+ * (last-bit differences); in split precision each tile also subtracts its own
+ * linear reference before rounding to FP32, so shapes agree to FP32 rounding
+ * of the residuals.  Pin one shape where results must match bit for bit. */
 int mcv_select_tile(mcv_handle *h, int index);
 
 /* Total mass and energy of `members` states that already live in the caller's
@@ -144,6 +165,10 @@ int mcv_grid_sizes(int order, int nc, int *npx, int *n, int *halo);
 
 /* Device bytes a handle with these arguments allocates (admission control). */
 long long mcv_footprint_bytes(int order, int nc, int scheme, int precision, int members);
+
+/* Free and total bytes of the current device (cudaMemGetInfo), for admission
+ * control by HBM footprint. */
+int mcv_device_memory(long long *free_bytes, long long *total_bytes);
 
 /* ---------------------------------------------------------------------
  * Host-side init chain (the caller's side of the boundary; provided so C,

@@ -20,6 +20,7 @@ _I = ctypes.POINTER(ctypes.c_int)
 
 RK3_TVD, RK4 = 3, 4
 FP64, MIXED = 0, 1
+BUSY, ERR_NONFINITE = 1, -5
 SCHEMES = {"RK3_TVD": RK3_TVD, "RK4": RK4}
 PRECISIONS = {"fp64": FP64, "mixed": MIXED}
 
@@ -55,6 +56,9 @@ def lib():
         "mcv_step": (ctypes.c_int, [vp, ctypes.c_int]),
         "mcv_step_async": (ctypes.c_int, [vp, ctypes.c_int]),
         "mcv_sync": (ctypes.c_int, [vp]),
+        "mcv_query": (ctypes.c_int, [vp]),
+        "mcv_set_active": (ctypes.c_int, [vp, ctypes.c_int, _I]),
+        "mcv_check_finite": (ctypes.c_int, [vp, _I]),
         "mcv_get_state": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
         "mcv_mass_energy": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
         "mcv_destroy": (ctypes.c_int, [vp]),
@@ -65,6 +69,7 @@ def lib():
         "mcv_mass_energy_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp,
                                                    vp, _D, _D]),
         "mcv_grid_sizes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _I, _I, _I]),
+        "mcv_device_memory": (ctypes.c_int, [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "mcv_footprint_bytes": (ctypes.c_longlong, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_int]),
         "mcv_build_geometry": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D, _D, _D, _D, _D,
@@ -116,6 +121,13 @@ def grid_sizes(order, nc):
 
 def footprint_bytes(order, nc, scheme="RK3_TVD", precision="fp64", members=1):
     return int(lib().mcv_footprint_bytes(int(order), int(nc), SCHEMES[scheme], PRECISIONS[precision], int(members)))
+
+
+def device_memory():
+    """(free, total) bytes of the current device."""
+    f, t = ctypes.c_longlong(), ctypes.c_longlong()
+    _check(lib().mcv_device_memory(ctypes.byref(f), ctypes.byref(t)))
+    return f.value, t.value
 
 
 class Geometry:
@@ -258,6 +270,27 @@ class Stepper:
     def sync(self):
         _check(lib().mcv_sync(self.h))
 
+    def query(self):
+        """True when all queued work has finished (never waits)."""
+        rc = lib().mcv_query(self.h)
+        if rc == BUSY:
+            return False
+        _check(rc)
+        return True
+
+    def set_active(self, members):
+        """Members the following steps advance (the others keep their state)."""
+        ids = np.ascontiguousarray(np.asarray(list(members), dtype=np.int32))
+        _check(lib().mcv_set_active(self.h, len(ids), ids.ctypes.data_as(_I) if len(ids) else None))
+
+    def check_finite(self):
+        """Per-member flags, True where the interior u, v or phi holds a NaN or Inf."""
+        flags = np.zeros(self.members, dtype=np.int32)
+        rc = lib().mcv_check_finite(self.h, flags.ctypes.data_as(_I))
+        if rc not in (0, ERR_NONFINITE):
+            _check(rc)
+        return flags.astype(bool)
+
     def get_state(self, m=0, out=None):
         shp = (6, self.npx, self.npx)
         out = out or {k: np.empty(shp) for k in ("u", "v", "phi", "phiG")}
@@ -280,12 +313,13 @@ class Stepper:
         return list(st)[:nst], ha.value
 
     def tuning(self):
-        """Autotuner record: list of ((cells_x, cells_y, threads, walk), ms per launch) and the chosen index."""
+        """Autotuner record: list of ((cells_x, cells_y, threads, walk, ctas_per_sm), ms per launch)
+        and the chosen index."""
         n, ch = ctypes.c_int(), ctypes.c_int()
-        shapes = (ctypes.c_int * 64)()
+        shapes = (ctypes.c_int * 80)()
         ms = (ctypes.c_float * 16)()
         _check(lib().mcv_tuning(self.h, ctypes.byref(n), ctypes.byref(ch), shapes, ms))
-        cands = [(tuple(shapes[4 * i: 4 * i + 4]), ms[i]) for i in range(n.value)]
+        cands = [(tuple(shapes[5 * i: 5 * i + 5]), ms[i]) for i in range(n.value)]
         return cands, ch.value
 
     def select_tile(self, index):

@@ -178,6 +178,16 @@ def serving_requests(seed=4, rate=20.0, count=64):
     return reqs
 
 
+def serving_dt(geom, cfl=0.45):
+    """Fixed dt of a serving grid (order, Nc): CFL `cfl` on the unperturbed
+    balanced flow (u0 = 38.6 m/s, alpha = 0.05).  A request's harmonics (RMS
+    10 m) raise the largest signal speed by far less than the margin to 0.5,
+    and a mountain lowers it."""
+    zw, mw, phi = api.tilted_zonal(geom, equator_gh0(38.6, geom.radius), 38.6, 0.05)
+    u, v = api.sphere_to_cov(geom, zw, mw)
+    return cfl_dt(geom, u, v, phi, cfl)
+
+
 def serving_state(geom, req, scheme="RK3_TVD"):
     rng = np.random.default_rng(req["seed"])
     zw, mw, phi, phis, meta = balanced_flow(geom, rng, 38.6, 0.05, 8, 10.0, mountain=req["mountain"])

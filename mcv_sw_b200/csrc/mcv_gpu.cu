@@ -114,7 +114,8 @@ struct mcv_handle {
   double *Y[3]{}, *A[3]{}, *B[3]{}, *acc[3]{};
   // split precision: FP64 state ping-pong S[cur], S[1-cur]; FP32 increments DA, DB
   double *S[2][3]{};
-  int cur = 0;
+  int cur = 0;             // buffer the next step reads
+  std::vector<int> mcur;   // buffer holding each member (members left out of steps keep theirs)
   float *DA[3]{}, *DB[3]{}, *facc[3]{};
   float *phis32 = nullptr;
   float4 *bnd32 = nullptr;
@@ -131,6 +132,11 @@ struct mcv_handle {
   bool geometry_set = false;
   std::vector<char> member_set;
   std::vector<long long> steps_done;
+  // members the step advances: device list [n_active] read by both kernels
+  int *active = nullptr;
+  std::vector<int> active_host;
+  int n_active = 0;
+  int *flags = nullptr;  // non-finite flags [members]
   std::vector<double> sqrtG_host;  // padded Fortran layout, for phiG on download
   // stage kernel chosen by the autotuner
   const StageLauncher *cands = nullptr;
@@ -159,7 +165,7 @@ struct Layout {
   size_t total = 0;
   size_t f64_state[9]{}, f64_acc[3]{}, mix_state[6]{}, mix_inc[6]{}, mix_acc[3]{};
   size_t metric[5]{}, phis = 0, phis32 = 0, bnd = 0, bnd32 = 0, M = 0, N = 0, iref = 0, coef = 0, partial = 0,
-         met1d = 0, phibar = 0;
+         met1d = 0, phibar = 0, active = 0, flags = 0;
 };
 
 Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int members) {
@@ -196,6 +202,8 @@ Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int memb
   L.iref = take(sizeof(int) * (size_t)H * g.n);
   L.coef = take(sizeof(double2) * (size_t)H * g.n);
   L.partial = take(sizeof(double4) * kPartialBlocks);
+  L.active = take(sizeof(int) * (size_t)members);
+  L.flags = take(sizeof(int) * (size_t)members);
   L.total = off;
   return L;
 }
@@ -232,6 +240,7 @@ StageArgs stage_args(mcv_handle *h, int s, int c) {
   a.sqrtG = h->sqrtG; a.ig11 = h->ig11; a.ig12 = h->ig12; a.ig22 = h->ig22; a.fcor = h->fcor;
   a.phis = h->phis;
   a.bnd = h->bnd;
+  a.active = h->active;
   const double dt = h->dt;
   const int kind = stage_kind(h, s);
   if (!h->mixed) {
@@ -287,7 +296,8 @@ HaloArgs halo_args(mcv_handle *h, int s, int c) {
   a.dx = h->g.dx;
   a.dx2 = h->dx2;
   a.dx3 = h->dx3;
-  a.members = h->members;
+  a.members = h->n_active;
+  a.active = h->active;
   const int kind = stage_kind(h, s);
   if (!h->mixed) {
     double *const *out = (kind == RK3_S1 || kind == RK4_S1 || kind == RK4_S3) ? h->A
@@ -310,7 +320,7 @@ HaloArgs halo_args(mcv_handle *h, int s, int c) {
 void launch_halo(mcv_handle *h, int s, int c) {
   const HaloArgs a = halo_args(h, s, c);
   const bool mixed_inc = h->mixed && !last_stage(stage_kind(h, s));
-  const long long threads = 24LL * (h->H + 1) * h->g.n * h->members;
+  const long long threads = 24LL * (h->H + 1) * h->g.n * h->n_active;
   const int block = 128;
   const unsigned grid = (unsigned)((threads + block - 1) / block);
   if (h->order == 3) {
@@ -326,7 +336,7 @@ void launch_stage(mcv_handle *h, const StageLauncher &L, int s, int c) {
   GridDesc g = h->g;
   g.tiles_x = (h->nc + L.CX - 1) / L.CX;
   g.tiles_y = (h->nc + L.CY - 1) / L.CY;
-  L.launch[stage_kind(h, s)](dim3(g.tiles_x * g.tiles_y, 6, h->members), h->stream, g, stage_args(h, s, c));
+  L.launch[stage_kind(h, s)](dim3(g.tiles_x * g.tiles_y, 6, h->n_active), h->stream, g, stage_args(h, s, c));
 }
 
 // Stage s of one RK step on every member: fused stage kernel, then the halo
@@ -393,12 +403,31 @@ int build_graphs(mcv_handle *h) {
   return MCV_OK;
 }
 
-int ready_to_step(mcv_handle *h) {
+// Checks the handle and lazily builds the step graphs.  With no active member
+// a step enqueues nothing (*idle); callers that need a launch pass no flag.
+int ready_to_step(mcv_handle *h, bool *idle = nullptr) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   if (!h->geometry_set) return fail(MCV_ERR_ORDER, "mcv_set_geometry must precede stepping");
-  for (int m = 0; m < h->members; ++m)
-    if (!h->member_set[m]) return fail(MCV_ERR_ORDER, "every member must be set before stepping");
+  for (int k = 0; k < h->n_active; ++k)
+    if (!h->member_set[h->active_host[k]])
+      return fail(MCV_ERR_ORDER, "every active member must be set before stepping");
+  if (h->n_active == 0) {
+    if (!idle) return fail(MCV_ERR_ORDER, "no active member");
+    *idle = true;
+    return MCV_OK;
+  }
+  if (idle) *idle = false;
   return build_graphs(h);
+}
+
+// After nsteps of the active members: their step counts, and (split
+// precision) the buffer now holding them.
+void count_steps(mcv_handle *h, int nsteps) {
+  for (int k = 0; k < h->n_active; ++k) {
+    const int m = h->active_host[k];
+    h->steps_done[m] += nsteps;
+    if (h->mixed) h->mcur[m] = h->cur;
+  }
 }
 
 // Enqueue nsteps replays of the step graph (split precision alternates the two).
@@ -407,12 +436,13 @@ int enqueue_steps(mcv_handle *h, int nsteps) {
     MCV_CUDA(cudaGraphLaunch(h->graph_exec[h->mixed ? h->cur : 0], h->stream), "launch step graph");
     if (h->mixed) h->cur = 1 - h->cur;
   }
-  for (int m = 0; m < h->members; ++m) h->steps_done[m] += nsteps;
+  count_steps(h, nsteps);
   return MCV_OK;
 }
 
 // The state arrays of the current step.
-double *const *state(mcv_handle *h) { return h->mixed ? h->S[h->cur] : h->Y; }
+// The state arrays holding member m.
+double *const *state(mcv_handle *h, int m) { return h->mixed ? h->S[h->mcur[m]] : h->Y; }
 
 }  // namespace
 
@@ -425,6 +455,15 @@ extern "C" long long mcv_footprint_bytes(int order, int nc, int scheme, int prec
   int H, npx;
   grid_desc(order, nc, g, H, npx);
   return (long long)make_layout(g, H, scheme, precision, members).total;
+}
+
+extern "C" int mcv_device_memory(long long *free_bytes, long long *total_bytes) {
+  if (!free_bytes || !total_bytes) return fail(MCV_ERR_ARG, "output is NULL");
+  size_t f = 0, t = 0;
+  MCV_CUDA(cudaMemGetInfo(&f, &t), "device memory");
+  *free_bytes = (long long)f;
+  *total_bytes = (long long)t;
+  return MCV_OK;
 }
 
 extern "C" int mcv_create(int order, int nc, int scheme, int precision, double dt, double radius, int members,
@@ -464,6 +503,7 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->dx3 = std::pow(h->g.dx, 3.);
   h->member_set.assign(members, 0);
   h->steps_done.assign(members, 0);
+  h->mcur.assign(members, 0);
   h->phibar_host.assign(members, 0.);
   h->cands = stage_launchers(order, h->mixed, &h->ncands);
   for (int i = 0; i < h->ncands; ++i) {
@@ -525,8 +565,16 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->giref = (int *)(base + L.iref);
   h->gcoef = (double2 *)(base + L.coef);
   h->partial = (double4 *)(base + L.partial);
+  h->active = (int *)(base + L.active);
+  h->flags = (int *)(base + L.flags);
   // zero everything once: unused pitch padding and halo corners stay finite
   e = cudaMemsetAsync(h->pool, 0, L.total, h->stream);
+  // every member is active until mcv_set_active says otherwise
+  h->active_host.resize(members);
+  for (int m = 0; m < members; ++m) h->active_host[m] = m;
+  h->n_active = members;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h->active, h->active_host.data(), sizeof(int) * members, cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     int r = cuda_fail(e, "clear device memory");
@@ -641,7 +689,8 @@ extern "C" int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const d
   if (!phi_s || !u || !v || !phi) return fail(MCV_ERR_ARG, "state array is NULL");
   if (!h->geometry_set) return fail(MCV_ERR_ORDER, "mcv_set_geometry must precede mcv_set_member");
   const long long off = (long long)m * h->g.mstride;
-  double *const *Y = state(h);
+  if (h->mixed) h->mcur[m] = h->cur;
+  double *const *Y = state(h, m);
   int rc;
   if ((rc = upload_padded(h, h->phis + off, phi_s, 8))) return rc;
   if ((rc = upload_padded(h, Y[0] + off, u, 8))) return rc;
@@ -676,13 +725,92 @@ extern "C" int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const d
 extern "C" int mcv_step_async(mcv_handle *h, int nsteps) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   if (nsteps < 0) return fail(MCV_ERR_ARG, "nsteps must be >= 0");
-  if (int rc = ready_to_step(h)) return rc;
+  bool idle = false;
+  if (int rc = ready_to_step(h, &idle)) return rc;
+  if (idle) return MCV_OK;
   return enqueue_steps(h, nsteps);
 }
 
 extern "C" int mcv_sync(mcv_handle *h) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   MCV_CUDA(cudaStreamSynchronize(h->stream), "step");
+  return MCV_OK;
+}
+
+extern "C" int mcv_query(mcv_handle *h) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  const cudaError_t e = cudaStreamQuery(h->stream);
+  if (e == cudaSuccess) return MCV_OK;
+  if (e == cudaErrorNotReady) {
+    cudaGetLastError();
+    return MCV_BUSY;
+  }
+  return cuda_fail(e, "query");
+}
+
+extern "C" int mcv_check_finite(mcv_handle *h, int *flags) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  MCV_CUDA(cudaMemsetAsync(h->flags, 0, sizeof(int) * h->members, h->stream), "clear flags");
+  for (int m = 0; m < h->members; ++m) {
+    // one launch per member: split-precision members may sit in different buffers
+    double *const *y = state(h, m);
+    const long long off = (long long)m * h->g.mstride;
+    finite_check_kernel<<<148, 256, 0, h->stream>>>(h->g, h->H, y[0] + off, y[1] + off, y[2] + off, h->flags + m);
+  }
+  MCV_CUDA(cudaGetLastError(), "launch finite check");
+  std::vector<int> f(h->members);
+  MCV_CUDA(cudaMemcpyAsync(f.data(), h->flags, sizeof(int) * h->members, cudaMemcpyDeviceToHost, h->stream),
+           "download flags");
+  MCV_CUDA(cudaStreamSynchronize(h->stream), "finite check");
+  if (flags)
+    for (int m = 0; m < h->members; ++m) flags[m] = f[m];
+  for (int k = 0; k < h->n_active; ++k)
+    if (f[h->active_host[k]]) return fail(MCV_ERR_NONFINITE, "an active member's state is not finite");
+  return MCV_OK;
+}
+
+extern "C" int mcv_set_active(mcv_handle *h, int count, const int *members) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (count < 0 || count > h->members) return fail(MCV_ERR_ARG, "active count out of range [0, members]");
+  if (count > 0 && !members) return fail(MCV_ERR_ARG, "members is NULL");
+  std::vector<char> seen(h->members, 0);
+  for (int k = 0; k < count; ++k) {
+    const int m = members[k];
+    if (m < 0 || m >= h->members) return fail(MCV_ERR_ARG, "active member index out of range");
+    if (seen[m]) return fail(MCV_ERR_ARG, "active member listed twice");
+    seen[m] = 1;
+  }
+  if (count != h->n_active) {
+    // the step graphs hold the launch grids: rebuild before the next step
+    MCV_CUDA(cudaStreamSynchronize(h->stream), "drain before changing the active set");
+    for (int c = 0; c < 2; ++c)
+      if (h->graph_exec[c]) {
+        cudaGraphExecDestroy(h->graph_exec[c]);
+        h->graph_exec[c] = nullptr;
+      }
+  }
+  for (int k = 0; k < count; ++k) {
+    const int m = members[k];
+    h->active_host[k] = m;
+    if (h->mixed && h->mcur[m] != h->cur) {
+      // a member left out of earlier steps sits in the other buffer: move it
+      // to the one the next step reads
+      const size_t bytes = (size_t)h->g.mstride * sizeof(double);
+      const long long off = (long long)m * h->g.mstride;
+      for (int f = 0; f < 3; ++f)
+        MCV_CUDA(cudaMemcpyAsync(h->S[h->cur][f] + off, h->S[h->mcur[m]][f] + off, bytes, cudaMemcpyDeviceToDevice,
+                                 h->stream),
+                 "move member state");
+      h->mcur[m] = h->cur;
+    }
+  }
+  h->n_active = count;
+  // ordered after the steps already enqueued on the handle's stream; a copy
+  // from pageable memory has consumed the host list when it returns
+  if (count > 0)
+    MCV_CUDA(cudaMemcpyAsync(h->active, h->active_host.data(), sizeof(int) * count, cudaMemcpyHostToDevice,
+                             h->stream),
+             "upload active members");
   return MCV_OK;
 }
 
@@ -702,7 +830,7 @@ extern "C" int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double 
     tmp.resize(NP);
     phi_dst = tmp.data();
   }
-  double *const *Y = state(h);
+  double *const *Y = state(h, m);
   int rc;
   if (u && (rc = download_padded(h, u, Y[0] + off))) return rc;
   if (v && (rc = download_padded(h, v, Y[1] + off))) return rc;
@@ -735,7 +863,7 @@ extern "C" int mcv_mass_energy(mcv_handle *h, int m, double *mass, double *energ
   if (!h->geometry_set || !h->member_set[m]) return fail(MCV_ERR_ORDER, "geometry and member must be set");
   const long long off = (long long)m * h->g.mstride;
   const double w0 = 1., w1 = (h->order == 3) ? 4. : 3., wden = (h->order == 3) ? 36. : 80.;
-  double *const *Y = state(h);
+  double *const *Y = state(h, m);
   if (h->order == 3)
     mass_energy_kernel<3><<<kPartialBlocks, 256, 0, h->stream>>>(h->g, Y[0] + off, Y[1] + off, Y[2] + off, h->sqrtG,
                                                                  h->ig11, h->ig12, h->ig22, h->phis + off, w0, w1,
@@ -819,7 +947,7 @@ extern "C" int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, dou
   if (err != cudaSuccess) return cuda_fail(err, "profiled steps");
   for (int s = 0; s < 4; ++s) stage_ms[s] = s < S ? st[s] / nsteps : 0.;
   *halo_ms = ha / ((double)nsteps * S);
-  for (int m = 0; m < h->members; ++m) h->steps_done[m] += nsteps;
+  count_steps(h, nsteps);
   return MCV_OK;
 }
 
@@ -829,10 +957,11 @@ extern "C" int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, f
   if (chosen) *chosen = h->choice;
   for (int i = 0; i < h->ncands; ++i) {
     if (shapes) {
-      shapes[4 * i] = h->cands[i].CX;
-      shapes[4 * i + 1] = h->cands[i].CY;
-      shapes[4 * i + 2] = h->cands[i].NT;
-      shapes[4 * i + 3] = h->cands[i].walk ? 1 : 0;
+      shapes[5 * i] = h->cands[i].CX;
+      shapes[5 * i + 1] = h->cands[i].CY;
+      shapes[5 * i + 2] = h->cands[i].NT;
+      shapes[5 * i + 3] = h->cands[i].walk ? 1 : 0;
+      shapes[5 * i + 4] = h->cands[i].minb;
     }
     if (ms) ms[i] = h->tune_ms[i];
   }

@@ -12,7 +12,8 @@ struct HaloArgs {
   const int *giref;           // ghost%iref [H][n] (1-based cell)
   const double2 *gcoef;       // {ghost%coef, ghost%coef**3.} [H][n]
   double dx, dx2, dx3;        // dx, dx**2., dx**3.
-  int members;
+  int members;                // active members in this launch
+  const int *active;          // member index of each active slot [members]
   // split precision: the field completed is Y + increment; u/v/phi above are
   // Y (read only), the increment's halo and boundary are written instead
   float *du, *dv, *dp;
@@ -85,8 +86,9 @@ __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloA
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long per_member = 24LL * (H + 1) * n;
   if (gid >= per_member * a.members) return;
-  const int mem = (int)(gid / per_member);
-  int rem = (int)(gid - (long long)mem * per_member);
+  const int slot = (int)(gid / per_member);
+  const int mem = __ldg(a.active + slot);
+  int rem = (int)(gid - (long long)slot * per_member);
   const int k = rem % n;
   rem /= n;
   const int h = rem % (H + 1);
@@ -259,6 +261,25 @@ __global__ void __launch_bounds__(256) mass_energy_kernel(const GridDesc g, cons
     __syncthreads();
   }
   if (threadIdx.x == 0) partial[blockIdx.x] = make_double4(red_m[0].s, red_m[0].c, red_e[0].s, red_e[0].c);
+}
+
+// Failure detection: flags[m] = 1 if an interior u, v or phi of member m is
+// NaN or Inf (flags cleared by the caller; racing stores write the same value).
+__global__ void __launch_bounds__(256) finite_check_kernel(const GridDesc g, int H, const double *u, const double *v,
+                                                           const double *phi, int *flags) {
+  const int m = blockIdx.y;
+  const int n = g.n;
+  const long long per = 6LL * n * n;
+  bool bad = false;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < per;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(k / ((long long)n * n));
+    const int rem = (int)(k - (long long)p * n * n);
+    const int j = rem / n, i = rem - j * n;
+    const long long o = (long long)m * g.mstride + p * g.plane + (long long)(j + H) * g.P + (i + H);
+    bad |= !isfinite(u[o]) || !isfinite(v[o]) || !isfinite(phi[o]);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) flags[m] = 1;
 }
 
 }  // namespace mcv

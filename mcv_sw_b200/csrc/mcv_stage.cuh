@@ -61,6 +61,7 @@ struct StageArgs {
   const double *phis;                               // [M][6][np][P]
   double4 *bnd;  // raw boundary copy [M][6][4][n] {u, v, phi, 0}
   double inc;    // dt or dt/2 (update_stat's inc_t) or the RK3 tendency weight
+  const int *active;  // member index of each grid z slice (the members this launch advances)
   // ---- split-precision policy ----
   const double *yu, *yv, *yp;  // FP64 state Y (RK base and stage-1 input), padded; the last
                                // stage writes Y + increment to uo/vo/po (the other state buffer)
@@ -241,22 +242,55 @@ struct Tile {
   static constexpr int XR = SGNY + TX * (CY + 1);
   static constexpr int YR = XR + 3 * I;
   static constexpr int TOTAL = YR + 3 * I;
-  // 1-D metric tables (split precision): [LX] and [LY] double4 after the R arrays
+  // split precision, after the R arrays: 1-D metric tables [LX] and [LY] double4,
+  // then the per-tile linear references of E, u, v: planes [3][3] double,
+  // reference-point values [3][3] double, slopes [2][3] float
   static constexpr size_t MET_OFF = ((size_t)TOTAL * sizeof(R) + 31) / 32 * 32;
+  static constexpr size_t PLANE_OFF = MET_OFF + (size_t)(LX + LY) * sizeof(double4);
   static constexpr size_t bytes(bool mixed) {
-    return mixed ? MET_OFF + (size_t)(LX + LY) * sizeof(double4) : (size_t)TOTAL * sizeof(R);
+    return mixed ? PLANE_OFF + 18 * sizeof(double) + 6 * sizeof(float) : (size_t)TOTAL * sizeof(R);
   }
   static_assert(LX % 2 == 1, "odd shared row length");
 };
 
-template <int D, int CX, int CY, int NT, int KIND, bool MIXED, bool WALK>
-__global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const StageArgs a) {
+// Split precision: the FP64 quantities of one loaded point.  q = {E - phibar,
+// u, v, phiG, phiG cU, phiG cV} are the fields the sweeps difference.
+struct MixPoint {
+  double q[6];
+  double sg, cu, cv, g11, g22, fc;
+};
+__device__ __forceinline__ void mix_point(MixPoint &o, const double4 mx, const double4 my, double u, double v,
+                                          double p, double phs, double phibar, int panel, double two_omega) {
+  // equiangular metric from the separable 1-D tables {tan, cos^2/R^2, sin cos/R,
+  // R/cos^2} (projection_mod.F90:150-211 with cos^2 y (1 + tan^2 y) = 1)
+  const double rho2 = 1. + mx.x * mx.x + my.x * my.x;
+  const double rinv = rsqrt(rho2);
+  o.sg = mx.w * my.w * (rinv * rinv * rinv);
+  o.g11 = rho2 * mx.y;
+  o.g22 = rho2 * my.y;
+  const double g12 = rho2 * (mx.z * my.z);
+  o.cu = o.g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
+  o.cv = g12 * u + o.g22 * v;
+  const double pg = p * o.sg;
+  o.q[0] = (p - phibar) + phs + 0.5 * (o.cu * u + o.cv * v);  // E = phi + phi_s + K
+  o.q[1] = u;
+  o.q[2] = v;
+  o.q[3] = pg;
+  o.q[4] = pg * o.cu;
+  o.q[5] = pg * o.cv;
+  // Coriolis f = 2 Omega sin(lat): sin(lat) = tan y / rho on panels 1-4, +-1/rho on 5, 6
+  o.fc = two_omega * (panel < 4 ? my.x * rinv : (panel == 4 ? rinv : -rinv));
+}
+
+// MINB: CTAs per SM the register allocation must allow (launch bounds).
+template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, bool WALK>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const StageArgs a) {
   using R = std::conditional_t<MIXED, float, double>;
   using T = Tile<D, CX, CY, R>;
   constexpr int H = T::H, LX = T::LX;
   extern __shared__ __align__(32) unsigned char smraw[];
   R *sm = reinterpret_cast<R *>(smraw);
-  const int tile = blockIdx.x, panel = blockIdx.y, mem = blockIdx.z;
+  const int tile = blockIdx.x, panel = blockIdx.y, mem = __ldg(a.active + blockIdx.z);
   const int tx = tile % g.tiles_x, ty = tile / g.tiles_x;
   const int c0x = tx * CX, c0y = ty * CY;
   const int ncx = min(CX, g.Nc - c0x), ncy = min(CY, g.Nc - c0y);
@@ -264,24 +298,28 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
   const int lxe = ncx * (D - 1) + 1 + 2 * H, lye = ncy * (D - 1) + 1 + 2 * H;
   const long long pbase = (long long)panel * g.plane;
   const long long mbase = (long long)mem * g.mstride + pbase;
-  const double4 *metx = reinterpret_cast<const double4 *>(smraw + T::MET_OFF);
-  const double4 *mety = metx + LX;
-
-  if constexpr (MIXED) {
-    // the tile's slices of the 1-D metric table
-    double4 *mx = reinterpret_cast<double4 *>(smraw + T::MET_OFF);
-    for (int k = threadIdx.x; k < LX + T::LY; k += NT) {
-      const int gidx = (k < LX) ? X0 + k : Y0 + (k - LX);
-      if (gidx < g.np) mx[k] = a.met1d[gidx];
-    }
-    __syncthreads();
-  }
+  const int txe = ncx * (D - 1) + 1, tye = ncy * (D - 1) + 1;  // tile points per row / column
   const double phibar = MIXED ? a.phibar[mem] : 0.;
+  double4 *metx = reinterpret_cast<double4 *>(smraw + T::MET_OFF);  // split precision: [LX] then [LY]
+  const double4 *mety = metx + LX;
+  double *plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF);  // [3] {value at (H, H), d/dlx, d/dly}
+  double *qref = plane + 9;                                            // [3 points][3]
+  float *slope = reinterpret_cast<float *>(qref + 9);                  // [x, y][3]: derivative per radian
 
   // ---- phase 0: load the tile and its halo cross, pointwise quantities ----
   // (spatial_operators_mod.F90:58-61, eigenvalues :248-280, upwind signs :83-85)
   // Per-tile base pointers: every field shares the pitch, so one 32-bit offset
   // per point addresses all of them.
+  // Split precision: E, u and v -- the fields of the momentum tendencies, whose
+  // pressure-gradient and Coriolis terms nearly cancel -- are formed in FP64,
+  // and a linear function of (lx, ly) fitted to three points of the tile is
+  // subtracted before rounding to FP32.  The reconstruction and the Riemann
+  // fluxes are linear in the fields and exact for linear data (equal one-sided
+  // derivatives, no jump), so the sweeps of the residual plus the plane's exact
+  // derivative equal the sweeps of the field, while FP32 holds only the
+  // residual's leading digits.  phiG and its fluxes are rounded as they are:
+  // both neighbours of a tile seam then see the same FP32 values, the seam
+  // fluxes agree bit for bit and the flux form keeps conserving mass.
   const long long tbase = (long long)Y0 * g.P + X0;
   const double *t_us = a.us + mbase + tbase, *t_vs = a.vs + mbase + tbase, *t_ps = a.ps + mbase + tbase;
   const double *t_ph = a.phis + mbase + tbase, *t_sg = a.sqrtG + pbase + tbase;
@@ -291,9 +329,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
   const float *t_p32 = a.phis32 + mbase + tbase;
   {
     constexpr int CH = 3;  // points per thread whose loads are in flight together
-    constexpr int NL = MIXED ? 7 : 8;
+    constexpr int NL = MIXED ? 3 : 8;
     for (int base = 0; base < T::A; base += NT * CH) {
       double r[NL][CH];
+      float f[4][CH];
       bool ok[CH];
 #pragma unroll
       for (int k = 0; k < CH; ++k) {
@@ -317,13 +356,52 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
             r[0][k] = __ldg(t_yu + o);
             r[1][k] = __ldg(t_yv + o);
             r[2][k] = __ldg(t_yp + o);
-            r[3][k] = (double)__ldg(t_p32 + o);
+            f[0][k] = __ldg(t_p32 + o);
             if constexpr (!first_stage(KIND)) {
-              r[4][k] = (double)__ldg(t_du + o);
-              r[5][k] = (double)__ldg(t_dv + o);
-              r[6][k] = (double)__ldg(t_dp + o);
+              f[1][k] = __ldg(t_du + o);
+              f[2][k] = __ldg(t_dv + o);
+              f[3][k] = __ldg(t_dp + o);
             }
           }
+        }
+      }
+      if constexpr (MIXED) {
+        if (base == 0) {  // block-uniform: runs once, while the first points' loads are in flight
+          for (int k = threadIdx.x; k < LX + T::LY; k += NT) {
+            const int gidx = (k < LX) ? X0 + k : Y0 + (k - LX);
+            if (gidx < g.np) metx[k] = a.met1d[gidx];
+          }
+          if (threadIdx.x < 3) {
+            // reference points (H, H), (txe - 1 + H, H), (H, tye - 1 + H): interior
+            const int lx = H + (threadIdx.x == 1 ? txe - 1 : 0), ly = H + (threadIdx.x == 2 ? tye - 1 : 0);
+            const int o = ly * g.P + lx;
+            double u = __ldg(t_yu + o), v = __ldg(t_yv + o), p = __ldg(t_yp + o);
+            if constexpr (!first_stage(KIND)) {
+              u += (double)__ldg(t_du + o);
+              v += (double)__ldg(t_dv + o);
+              p += (double)__ldg(t_dp + o);
+            }
+            MixPoint mp;
+            mix_point(mp, a.met1d[X0 + lx], a.met1d[Y0 + ly], u, v, p, (double)__ldg(t_p32 + o), phibar, panel,
+                      a.two_omega);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) qref[threadIdx.x * 3 + q] = mp.q[q];
+          }
+          __syncthreads();
+          if (threadIdx.x < 3) {
+            // The derivative added back is FP32, so the plane takes its slope
+            // from the rounded value: the two agree to FP64 rounding.
+            const int q = threadIdx.x;
+            const double q0 = qref[q];
+            const float sx = (float)((qref[3 + q] - q0) / ((double)ncx * g.dx));
+            const float sy = (float)((qref[6 + q] - q0) / ((double)ncy * g.dx));
+            plane[3 * q] = q0;
+            plane[3 * q + 1] = (double)sx * (g.dx / (double)(D - 1));  // per point index
+            plane[3 * q + 2] = (double)sy * (g.dx / (double)(D - 1));
+            slope[q] = sx;
+            slope[3 + q] = sy;
+          }
+          __syncthreads();
         }
       }
 #pragma unroll
@@ -331,42 +409,48 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
         if (!ok[k]) continue;
         const int idx = base + threadIdx.x + k * NT;
         const int ly = idx / LX, lx = idx - ly * LX;
-        R u, v, phi, dev, phs, sg, g11, g12, g22, pg, fc = R(0);
+        R u, v, phi, sg, g11, g22, cu, cv, fc = R(0);
         if constexpr (!MIXED) {
-          u = r[0][k]; v = r[1][k]; phi = r[2][k]; dev = phi; phs = r[3][k];
-          sg = r[4][k]; g11 = r[5][k]; g12 = r[6][k]; g22 = r[7][k];
-          pg = phi * sg;
+          u = r[0][k]; v = r[1][k]; phi = r[2][k];
+          const double phs = r[3][k];
+          sg = r[4][k]; g11 = r[5][k];
+          const double g12 = r[6][k];
+          g22 = r[7][k];
+          const double pg = phi * sg;
+          cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
+          cv = g12 * u + g22 * v;
+          sm[T::U + idx] = u;
+          sm[T::V + idx] = v;
+          sm[T::PG + idx] = pg;
+          sm[T::PGU + idx] = pg * cu;
+          sm[T::PGV + idx] = pg * cv;
+          sm[T::E + idx] = phi + phs + 0.5 * (cu * u + cv * v);  // E = phi + phi_s + K
         } else {
           double u64 = r[0][k], v64 = r[1][k], p64 = r[2][k];
           if constexpr (!first_stage(KIND)) {
-            u64 += r[4][k];
-            v64 += r[5][k];
-            p64 += r[6][k];
+            u64 += (double)f[1][k];
+            v64 += (double)f[2][k];
+            p64 += (double)f[3][k];
           }
-          // equiangular metric from the separable 1-D tables, in FP64
-          // (projection_mod.F90:150-211 with cos^2 y (1 + tan^2 y) = 1)
-          const double4 mx = metx[lx], my = mety[ly];
-          const double rho2 = 1. + mx.x * mx.x + my.x * my.x;
-          const double rinv = rsqrt(rho2);
-          const double sg64 = mx.w * my.w * (rinv * rinv * rinv);
-          u = (R)u64; v = (R)v64; phi = (R)p64; dev = (R)(p64 - phibar); phs = (R)r[3][k];
-          sg = (R)sg64;
-          g11 = (R)(rho2 * mx.y);
-          g22 = (R)(rho2 * my.y);
-          g12 = (R)(rho2 * (mx.z * my.z));
-          pg = (R)(p64 * sg64);
-          // Coriolis f = 2 Omega sin(lat): sin(lat) = tan y / rho on panels 1-4, +-1/rho on 5, 6
-          fc = (R)(a.two_omega * (panel < 4 ? my.x * rinv : (panel == 4 ? rinv : -rinv)));
+          MixPoint mp;
+          mix_point(mp, metx[lx], mety[ly], u64, v64, p64, (double)f[0][k], phibar, panel, a.two_omega);
+          const double X = (double)(lx - H), Y = (double)(ly - H);
+          sm[T::E + idx] = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
+          sm[T::U + idx] = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
+          sm[T::V + idx] = (float)(mp.q[2] - (plane[6] + plane[7] * X + plane[8] * Y));
+          sm[T::PG + idx] = (float)mp.q[3];
+          sm[T::PGU + idx] = (float)mp.q[4];
+          sm[T::PGV + idx] = (float)mp.q[5];
+          u = (R)u64;
+          v = (R)v64;
+          phi = (R)p64;
+          sg = (R)mp.sg;
+          g11 = (R)mp.g11;
+          g22 = (R)mp.g22;
+          cu = (R)mp.cu;
+          cv = (R)mp.cv;
+          fc = (R)mp.fc;
         }
-        const R cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
-        const R cv = g12 * u + g22 * v;
-        const R K = R(0.5) * (cu * u + cv * v);
-        sm[T::U + idx] = u;
-        sm[T::V + idx] = v;
-        sm[T::PG + idx] = pg;
-        sm[T::PGU + idx] = pg * cu;
-        sm[T::PGV + idx] = pg * cv;
-        sm[T::E + idx] = dev + phs + K;  // E = phi + phi_s + K (MIXED: phi - phibar; constants drop out of d/dx)
         const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
         if (!xh && !yh) {
           const int ix = lx - H, iy = ly - H;
@@ -389,8 +473,6 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
     }
   }
   __syncthreads();
-
-  const int txe = ncx * (D - 1) + 1, tye = ncy * (D - 1) + 1;
   const Widths<R> w(g);
 
   if constexpr (!WALK) {
@@ -478,8 +560,16 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
     const R sg = sm[T::SG + it], cu = sm[T::CU + it], cv = sm[T::CV + it];
     const R fc = MIXED ? sm[T::FC + it] : (R)__ldg(a.fcor + pbase + tbase + ((H + r) * g.P + (H + q)));
     const R rsg = R(1) / sg;
-    const R flux_x = sm[T::XR + it], div_x = sm[T::XR + T::I + it], dvdx = sm[T::XR + 2 * T::I + it];
-    const R flux_y = sm[T::YR + it], div_y = sm[T::YR + T::I + it], dudy = sm[T::YR + 2 * T::I + it];
+    R flux_x = sm[T::XR + it], dvdx = sm[T::XR + 2 * T::I + it];
+    R flux_y = sm[T::YR + it], dudy = sm[T::YR + 2 * T::I + it];
+    const R div_x = sm[T::XR + T::I + it], div_y = sm[T::YR + T::I + it];
+    if constexpr (MIXED) {
+      // the linear references' exact derivatives: E and v along x, E and u along y
+      flux_x += slope[0];
+      dvdx += slope[2];
+      flux_y += slope[3 + 0];
+      dudy += slope[3 + 1];
+    }
     const R vort = (dvdx - dudy) * rsg;
     const R tP = -div_x - div_y;
     const R tU = -flux_x + sg * (vort + fc) * cv;
@@ -599,25 +689,29 @@ __global__ void __launch_bounds__(NT) stage_kernel(const GridDesc g, const Stage
 using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a);
 
 struct StageLauncher {
-  int CX, CY, NT;
+  int CX, CY, NT, minb;
   bool walk;  // sweeps as line walks instead of per-cell items
   size_t smem;
   StageLaunchFn launch[7];  // indexed by StageKind
-  cudaError_t (*prepare)(); // raises the dynamic shared-memory limit of every kind
+  cudaError_t (*prepare)(); // shared-memory limit and carveout of every kind
 };
 
-template <int D, int CX, int CY, int NT, bool MIXED, bool WALK>
+template <int D, int CX, int CY, int NT, int MINB, bool MIXED, bool WALK>
 struct StageConfig {
   using T = Tile<D, CX, CY, std::conditional_t<MIXED, float, double>>;
   static constexpr size_t SMEM = T::bytes(MIXED);
   template <int KIND>
   static void launch(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a) {
-    stage_kernel<D, CX, CY, NT, KIND, MIXED, WALK><<<grid, NT, SMEM, s>>>(g, a);
+    stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK><<<grid, NT, SMEM, s>>>(g, a);
   }
   template <int KIND>
   static cudaError_t attr() {
-    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, KIND, MIXED, WALK>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    if (e != cudaSuccess) return e;
+    // the largest shared-memory carveout, so that MINB tiles fit on an SM
+    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK>,
+                                cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   }
   static cudaError_t prepare() {
     cudaError_t e;
@@ -628,7 +722,8 @@ struct StageConfig {
   }
   static StageLauncher make() {
     static_assert(SMEM <= 227 * 1024, "tile does not fit in shared memory");
-    return StageLauncher{CX, CY, NT, WALK, SMEM,
+    static_assert(MINB * (SMEM + 1024) <= 228 * 1024, "MINB tiles do not fit in one SM's shared memory");
+    return StageLauncher{CX, CY, NT, MINB, WALK, SMEM,
                          {&launch<0>, &launch<1>, &launch<2>, &launch<3>, &launch<4>, &launch<5>, &launch<6>},
                          &prepare};
   }

@@ -14,7 +14,7 @@ from tests.helpers import GRAVITY
 
 pytestmark = pytest.mark.gpu
 
-WALK_TOL = 1e-5  # FP32 rounding of differently contracted sums
+TILE_TOL = 1e-6  # FP32 rounding of other per-tile residuals, after 3 steps
 
 
 def normalized_l2(geom, a, b):
@@ -58,7 +58,10 @@ def test_mixed_one_day_error_bound():
     assert abs(drift) < 1e-9, drift
 
 
-def test_mixed_every_tile_shape_is_bit_identical():
+def test_mixed_tile_shapes_agree():
+    """Each tile subtracts its own linear reference before rounding to FP32, so
+    tile shapes agree to FP32 rounding of the residuals (not bit for bit), and a
+    shape run twice gives identical bits."""
     geom = api.Geometry(4, 20, cases.EARTH_RADIUS)
     st = cases.finish(geom, *cases.balanced_flow(geom, np.random.default_rng(5))[:4], "RK3_TVD", nsteps=3)
     outs = []
@@ -66,18 +69,16 @@ def test_mixed_every_tile_shape_is_bit_identical():
         s.set_geometry(geom)
         s.set_member(0, st.phi_s, st.u, st.v, st.phi)
         cands, _ = s.tuning()
-        for i in range(len(cands)):
+        for i in list(range(len(cands))) + [0]:
             s.select_tile(i)
             s.set_member(0, st.phi_s, st.u, st.v, st.phi)
             s.step(3)
             outs.append(s.get_state(0))
-    # per-cell-item shapes share one code path: bit-identical; line walks form the
-    # same sums with another FMA contraction
-    item = [i for i, (c, _) in enumerate(cands) if c[3] == 0]
-    for i in range(len(outs)):
+    for k in ("u", "v", "phi"):
+        assert np.array_equal(outs[-1][k], outs[0][k]), k
+    H, n = geom.H, geom.n
+    for i in range(1, len(outs) - 1):
         for k in ("u", "v", "phi"):
-            if i in item:
-                assert np.array_equal(outs[i][k], outs[item[0]][k]), (i, k)
-            else:
-                d = np.abs(outs[i][k] - outs[item[0]][k]).max() / np.abs(outs[item[0]][k]).max()
-                assert d < WALK_TOL, (i, k, d)
+            a, b = outs[i][k][:, H:H + n, H:H + n], outs[0][k][:, H:H + n, H:H + n]
+            d = np.abs(a - b).max() / np.abs(b).max()
+            assert d < TILE_TOL, (i, k, d)

@@ -1,0 +1,157 @@
+"""Host logic of the request loop (admission by footprint, chunking, slot
+reuse, eviction) with a stand-in for the device handle: each member's "state"
+counts the steps it was advanced, so a forecast that is stepped too far or
+too little shows up exactly."""
+import numpy as np
+import pytest
+
+from mcv_sw_b200 import serving
+
+
+class FakeStepper:
+    """Device handle stand-in: a chunk completes after two polls."""
+    created = []
+
+    def __init__(self, order, nc, dt, scheme, members=1, precision="mixed", radius=1.0):
+        self.members = members
+        self.steps = np.zeros(members, dtype=np.int64)
+        self.seed = np.full(members, -1.0)
+        self.active = list(range(members))
+        self.busy = 0
+        self.closed = False
+        FakeStepper.created.append(self)
+
+    def set_geometry(self, geom):
+        pass
+
+    def select_tile(self, i):
+        pass
+
+    def set_member(self, m, phi_s, u, v, phi):
+        assert not self.busy, "member upload while a chunk is in flight"
+        self.seed[m] = phi.flat[0]
+        self.steps[m] = 0
+
+    def set_active(self, members):
+        assert not self.busy, "active set changed while a chunk is in flight"
+        assert len(set(members)) == len(members)
+        self.active = list(members)
+
+    def step_async(self, k):
+        assert not self.busy and k >= 1
+        self.busy = 2
+        self.pending = k
+
+    def step(self, k):
+        self.step_async(k)
+        while not self.query():
+            pass
+
+    def query(self):
+        if self.busy:
+            self.busy -= 1
+            if self.busy == 0:
+                for m in self.active:
+                    self.steps[m] += self.pending
+        return self.busy == 0
+
+    def check_finite(self):
+        assert not self.busy
+        return np.zeros(self.members, dtype=bool)
+
+    def get_state(self, m):
+        assert not self.busy
+        return {"seed": self.seed[m], "steps": int(self.steps[m])}
+
+    def close(self):
+        self.closed = True
+
+
+def fake_footprint(order, nc, scheme, precision, members):
+    return (1000 + 100 * members) * nc
+
+
+def requests(specs):
+    out = []
+    for i, (t, order, nc, hours) in enumerate(specs):
+        phi = np.full((6, 4, 4), float(i))
+        out.append(serving.Request(i, t, order, nc, hours, phi * 0, phi * 0, phi * 0, phi))
+    return out
+
+
+def server(**kw):
+    FakeStepper.created = []
+    kw.setdefault("hbm_budget", 10 ** 9)
+    return serving.ForecastServer(stepper_factory=FakeStepper, footprint_fn=fake_footprint, keep_states=True,
+                                  poll_s=0.0, slot_bytes=300 * 8, chunk_ms=1e-3, **kw)
+
+
+def test_every_request_gets_exactly_its_steps():
+    reqs = requests([(0.0, 3, 8, 2.0), (0.0, 3, 8, 5.0), (0.001, 4, 8, 3.0), (0.002, 3, 8, 1.0),
+                     (0.002, 3, 12, 4.0), (0.003, 4, 8, 6.0), (0.003, 3, 8, 2.5)])
+    srv = server()
+    res = srv.run(reqs)
+    assert [r.id for r in res] == [q.id for q in reqs]
+    for q, r in zip(reqs, res):
+        assert r.state["seed"] == q.phi.flat[0]  # its own slot
+        assert r.state["steps"] == r.nsteps == srv.nsteps(q)
+        assert r.finished >= r.admitted >= r.arrival
+    # 3 slots per (3, 8) pool (slot_bytes / per-member bytes): one or two pools
+    # for its four requests (a slot may free up before the fourth arrives), one
+    # each for (4, 8) and (3, 12)
+    assert 3 <= srv.stats["pools_created"] <= 4
+
+
+def test_slots_are_reused_and_pools_added_when_full():
+    # slot_bytes 300*8 with footprint 100*nc per member -> 3 slots per pool at nc=8
+    reqs = requests([(0.0, 3, 8, 1.0 + k) for k in range(7)])
+    srv = server()
+    res = srv.run(reqs)
+    assert all(r.state["steps"] == r.nsteps for r in res)
+    assert srv.stats["pools_created"] == 3  # 7 concurrent requests / 3 slots
+    assert srv.slots_for((3, 8)) == 3
+
+
+def test_admission_waits_for_budget_and_evicts_idle_pools():
+    # budget for one pool only: the Nc=12 request waits until the Nc=8 pool has
+    # drained, which is then evicted to make room
+    one = fake_footprint(3, 12, None, None, 3)
+    reqs = requests([(0.0, 3, 8, 3.0), (0.0, 3, 12, 1.0)])
+    srv = server(hbm_budget=one)
+    res = srv.run(reqs)
+    assert all(r.state["steps"] == r.nsteps for r in res)
+    assert res[1].admitted >= res[0].finished - 1e-9
+    assert srv.stats["pools_evicted"] == 1
+    assert FakeStepper.created[0].closed
+
+
+def test_summary():
+    reqs = requests([(0.0, 3, 8, 2.0), (0.0, 3, 8, 4.0)])
+    s = serving.summarize(server().run(reqs))
+    assert s["requests"] == 2 and s["all_finite"]
+    assert s["p99_latency_s"] >= s["p50_latency_s"] > 0
+    assert s["sim_days_per_s"] > 0
+
+
+def test_request_stream_matches_configuration():
+    reqs = serving.cases.serving_requests(seed=4, count=400)
+    t = np.array([r["t"] for r in reqs])
+    assert np.all(np.diff(t) > 0)
+    assert abs(len(reqs) / t[-1] - 20.0) < 3.0  # Poisson rate 20/s
+    ncs = np.array([r["nc"] for r in reqs])
+    for nc, p in ((48, 0.4), (96, 0.3), (192, 0.2), (384, 0.1)):
+        assert abs(np.mean(ncs == nc) - p) < 0.07
+    hours = np.array([r["hours"] for r in reqs])
+    assert hours.min() >= 6.0 and hours.max() <= 120.0
+    assert abs(np.mean([r["order"] == 3 for r in reqs]) - 0.5) < 0.08
+    assert abs(np.mean([r["mountain"] for r in reqs]) - 0.5) < 0.08
+
+
+@pytest.mark.parametrize("order,nc", [(3, 8), (4, 12)])
+def test_serving_dt_is_below_the_cfl_limit(order, nc):
+    from mcv_sw_b200 import api, cases
+    g = api.Geometry(order, nc, cases.EARTH_RADIUS)
+    dt = cases.serving_dt(g)
+    for seed in range(3):
+        st = cases.serving_state(g, dict(seed=seed, mountain=bool(seed % 2), hours=6.0))
+        assert dt <= cases.cfl_dt(g, st.u, st.v, st.phi, 0.5)
