@@ -210,6 +210,13 @@ int mcv_ic_add_mountain(long long npts, const double *lonP, const double *latP, 
 int mcv_ic_add_rossby_haurwitz(long long npts, const double *lonP, const double *latP, double radius, int R,
                                double omg, double *zonal, double *merid, double *phi);
 
+/* Adds one linear Rossby wave of zonal wavenumber R and amplitude K (1/s):
+ * the wave part of the case-6 velocity (src/test_case_mod.F90:144-149)
+ * without its solid-body rotation, and the cos(R lon) height term balancing
+ * it at linear order (:160-164 with omega -> 0 in the factor Omega + omega). */
+int mcv_ic_add_rossby_wave(long long npts, const double *lonP, const double *latP, double radius, int R, double K,
+                           double *zonal, double *merid, double *phi);
+
 /* Covariant winds from sphere winds, (u,v) = (G IA)(zonal, merid), as
  * initTestCase does (src/test_case_mod.F90:32-39, projection_mod.F90:60-77). */
 int mcv_sphere_to_cov(long long npts, const double *matrixG, const double *matrixIA, const double *zonal,

@@ -83,6 +83,8 @@ def lib():
                                                ctypes.c_double, ctypes.c_double, ctypes.c_double, _D, _D]),
         "mcv_ic_add_rossby_haurwitz": (ctypes.c_int, [ctypes.c_longlong, _D, _D, ctypes.c_double, ctypes.c_int,
                                                       ctypes.c_double, _D, _D, _D]),
+        "mcv_ic_add_rossby_wave": (ctypes.c_int, [ctypes.c_longlong, _D, _D, ctypes.c_double, ctypes.c_int,
+                                                  ctypes.c_double, _D, _D, _D]),
         "mcv_sphere_to_cov": (ctypes.c_int, [ctypes.c_longlong, _D, _D, _D, _D, _D, _D]),
     }
     for name, (res, args) in sig.items():
@@ -202,6 +204,11 @@ def add_mountain(geom, phi, phis, lon_c, lat_c, h0=2000.0, efold=1.0e6):
 def add_rossby_haurwitz(geom, zw, mw, phi, wavenumber, omg):
     _check(lib().mcv_ic_add_rossby_haurwitz(geom.npts, _dp(geom.lonP), _dp(geom.latP), geom.radius, int(wavenumber),
                                             float(omg), _dp(zw), _dp(mw), _dp(phi)))
+
+
+def add_rossby_wave(geom, zw, mw, phi, wavenumber, K):
+    _check(lib().mcv_ic_add_rossby_wave(geom.npts, _dp(geom.lonP), _dp(geom.latP), geom.radius, int(wavenumber),
+                                        float(K), _dp(zw), _dp(mw), _dp(phi)))
 
 
 def sphere_to_cov(geom, zw, mw):

@@ -140,21 +140,21 @@ def ensemble_member(geom, seed, scheme="RK4", days=2.0):
 
 
 def stress(seed=5, nc=1024, order=4, scheme="RK4", nsteps=200, geom=None):
+    """Balanced zonal flow plus seeded linear Rossby waves of zonal wavenumber
+    4..12, each with a cos(R lon) height amplitude uniform in 50-200 m."""
     geom = geom or api.Geometry(order, nc, EARTH_RADIUS)
     rng = np.random.default_rng(seed)
     zw, mw, phi = api.tilted_zonal(geom, equator_gh0(38.6, geom.radius), 38.6, 0.05)
     phis = np.zeros(geom.shape)
     waves = []
+    t = np.linspace(-np.pi / 2, np.pi / 2, 2001)
     for R in range(4, 13):
         amp = rng.uniform(50.0, 200.0)
-        # angular velocity giving a height amplitude ~amp for wave number R
-        c = max(abs(np.cos(t) ** R * ((R * R + 2 * R + 2) - (R + 1) ** 2 * np.cos(t) ** 2))
-                for t in np.linspace(-1.5, 1.5, 301))
-        omg = amp * GRAVITY * (R + 1) * (R + 2) / (2.0 * 7.292e-5 * geom.radius ** 2 * c)
-        api.add_rossby_haurwitz(geom, zw, mw, phi, R, omg)
+        # K giving a height amplitude `amp`: max over latitude of the balanced term
+        c = np.abs(np.cos(t) ** R * ((R * R + 2 * R + 2) - (R + 1) ** 2 * np.cos(t) ** 2)).max()
+        K = amp * GRAVITY * (R + 1) * (R + 2) / (2.0 * 7.292e-5 * geom.radius ** 2 * c)
+        api.add_rossby_wave(geom, zw, mw, phi, R, K)
         waves.append((R, amp))
-    # the helper adds each wave's zonal-mean geopotential too; keep the mean depth
-    phi += GH0 - area_mean(geom, phi)
     return finish(geom, zw, mw, phi, phis, scheme, nsteps=nsteps, meta={"waves": waves}), geom
 
 

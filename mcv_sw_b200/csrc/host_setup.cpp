@@ -326,6 +326,24 @@ extern "C" int mcv_ic_add_rossby_haurwitz(long long npts, const double *lonP, co
   return MCV_OK;
 }
 
+extern "C" int mcv_ic_add_rossby_wave(long long npts, const double *lonP, const double *latP, double radius,
+                                      int Ri, double K, double *zonal, double *merid, double *phi) {
+  if (!lonP || !latP || !zonal || !merid || !phi || Ri < 1) return mcv::fail(MCV_ERR_ARG, "bad Rossby wave arguments");
+  const double R = Ri;
+#pragma omp parallel for schedule(static)
+  for (long long k = 0; k < npts; ++k) {
+    const double sl = std::sin(latP[k]), cl = std::cos(latP[k]), lon = lonP[k];
+    const double cR1 = std::pow(cl, R - 1), cR = cR1 * cl;
+    // the wave part of the case-6 velocity, without the solid-body rotation
+    zonal[k] += radius * K * cR1 * (R * sq(sl) - sq(cl)) * std::cos(R * lon);
+    merid[k] += -radius * K * R * cR1 * sl * std::sin(R * lon);
+    // its cos(R lon) height term at linear order in K (Coriolis balance)
+    const double B = 2. * kOmega * K / ((R + 1.) * (R + 2.)) * cR * ((sq(R) + 2. * R + 2.) - sq(R + 1.) * sq(cl));
+    phi[k] += sq(radius) * B * std::cos(R * lon);
+  }
+  return MCV_OK;
+}
+
 extern "C" int mcv_sphere_to_cov(long long npts, const double *matrixG, const double *matrixIA, const double *zonal,
                                  const double *merid, double *u, double *v) {
   if (!matrixG || !matrixIA || !zonal || !merid || !u || !v) return mcv::fail(MCV_ERR_ARG, "null array");

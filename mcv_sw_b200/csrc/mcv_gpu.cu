@@ -5,8 +5,11 @@
 // captured into a CUDA graph and replayed per step.  The stage kernel's tile
 // shape is chosen per handle by timing every candidate shape on the handle's
 // own grid before the first step (the autotuner).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -137,6 +140,10 @@ struct mcv_handle {
   std::vector<int> active_host;
   int n_active = 0;
   int *flags = nullptr;  // non-finite flags [members]
+  int *err = nullptr;    // stage-kernel error flag (TMA staging timed out)
+  int nsm = 0;           // SMs of the device
+  std::vector<int> bps;  // resident CTAs per SM of each candidate
+  int launch_err = 0;    // status of the last stage launch (tensor-map encoding)
   std::vector<double> sqrtG_host;  // padded Fortran layout, for phiG on download
   // stage kernel chosen by the autotuner
   const StageLauncher *cands = nullptr;
@@ -165,7 +172,7 @@ struct Layout {
   size_t total = 0;
   size_t f64_state[9]{}, f64_acc[3]{}, mix_state[6]{}, mix_inc[6]{}, mix_acc[3]{};
   size_t metric[5]{}, phis = 0, phis32 = 0, bnd = 0, bnd32 = 0, M = 0, N = 0, iref = 0, coef = 0, partial = 0,
-         met1d = 0, phibar = 0, active = 0, flags = 0;
+         met1d = 0, phibar = 0, active = 0, flags = 0, err = 0;
 };
 
 Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int members) {
@@ -204,6 +211,7 @@ Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int memb
   L.partial = take(sizeof(double4) * kPartialBlocks);
   L.active = take(sizeof(int) * (size_t)members);
   L.flags = take(sizeof(int) * (size_t)members);
+  L.err = take(sizeof(int));
   L.total = off;
   return L;
 }
@@ -241,6 +249,7 @@ StageArgs stage_args(mcv_handle *h, int s, int c) {
   a.phis = h->phis;
   a.bnd = h->bnd;
   a.active = h->active;
+  a.err = h->err;
   const double dt = h->dt;
   const int kind = stage_kind(h, s);
   if (!h->mixed) {
@@ -332,19 +341,88 @@ void launch_halo(mcv_handle *h, int s, int c) {
   }
 }
 
-void launch_stage(mcv_handle *h, const StageLauncher &L, int s, int c) {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+
+// Tensor map of one padded field seen as a 2-D array [rows][P] (rows = all
+// panels of all members, or of the one metric plane), box [box_y][box_x].
+int encode_field(CUtensorMap *m, const void *base, bool f32, const GridDesc &g, long long rows, int box_x,
+                 int box_y) {
+  auto fn = encode_fn();
+  if (!fn) return fail(MCV_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[2] = {(cuuint64_t)g.P, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)g.P * (f32 ? 4u : 8u)};
+  const cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)box_y};
+  const cuuint32_t es[2] = {1, 1};
+  const CUresult r = fn(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                        const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(MCV_ERR_CUDA, "tensor map encoding failed");
+  return MCV_OK;
+}
+
+// Tensor maps of the fields a TMA-form stage launch stages (the kernel's order).
+int stage_maps(mcv_handle *h, const StageLauncher &L, const StageArgs &a, int kind, TileMaps &tm) {
+  const long long per_member = (long long)h->members * 6 * h->g.np, plane = 6LL * h->g.np;
+  const int bx = L.box_x, by = L.box_y;
+  int rc;
+  if (!h->mixed) {
+    const double *f[8] = {a.us, a.vs, a.ps, a.phis, a.sqrtG, a.ig11, a.ig12, a.ig22};
+    for (int k = 0; k < 8; ++k)
+      if ((rc = encode_field(&tm.f[k], f[k], false, h->g, k < 4 ? per_member : plane, bx, by))) return rc;
+    return MCV_OK;
+  }
+  const double *f64[3] = {a.yu, a.yv, a.yp};
+  for (int k = 0; k < 3; ++k)
+    if ((rc = encode_field(&tm.f[k], f64[k], false, h->g, per_member, bx, by))) return rc;
+  if ((rc = encode_field(&tm.f[3], a.phis32, true, h->g, per_member, bx, by))) return rc;
+  if (!first_stage(kind)) {
+    const float *f32[3] = {a.du, a.dv, a.dp};
+    for (int k = 0; k < 3; ++k)
+      if ((rc = encode_field(&tm.f[4 + k], f32[k], true, h->g, per_member, bx, by))) return rc;
+  }
+  return MCV_OK;
+}
+
+int launch_stage(mcv_handle *h, int cand, int s, int c) {
+  const StageLauncher &L = h->cands[cand];
   GridDesc g = h->g;
   g.tiles_x = (h->nc + L.CX - 1) / L.CX;
   g.tiles_y = (h->nc + L.CY - 1) / L.CY;
-  L.launch[stage_kind(h, s)](dim3(g.tiles_x * g.tiles_y, 6, h->n_active), h->stream, g, stage_args(h, s, c));
+  const StageArgs a = stage_args(h, s, c);
+  const int kind = stage_kind(h, s);
+  TileMaps tm;
+  std::memset(&tm, 0, sizeof(tm));
+  if (!L.tma) {
+    L.launch[kind](dim3(g.tiles_x * g.tiles_y, 6, h->n_active), h->stream, g, a, tm);
+    return MCV_OK;
+  }
+  if (int rc = stage_maps(h, L, a, kind, tm)) return rc;
+  tm.total = g.tiles_x * g.tiles_y * 6 * h->n_active;
+  const int ctas = std::max(1, std::min(tm.total, h->bps[cand] * h->nsm));
+  L.launch[kind](dim3(ctas), h->stream, g, a, tm);
+  return MCV_OK;
 }
 
 // Stage s of one RK step on every member: fused stage kernel, then the halo
 // kernel on the stage's output.
-void enqueue_stage(mcv_handle *h, int s, int c, cudaEvent_t mid = nullptr) {
-  launch_stage(h, h->cands[h->choice], s, c);
+int enqueue_stage(mcv_handle *h, int s, int c, cudaEvent_t mid = nullptr) {
+  if (int rc = launch_stage(h, h->choice, s, c)) return rc;
   if (mid) cudaEventRecord(mid, h->stream);
   launch_halo(h, s, c);
+  return MCV_OK;
 }
 
 // Time every candidate tile shape on this grid with the second stage kind,
@@ -359,10 +437,14 @@ int autotune(mcv_handle *h) {
   int besti = 0;
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < h->ncands && e == cudaSuccess; ++i) {
-    const StageLauncher &L = h->cands[i];
-    launch_stage(h, L, 1, h->cur);  // warm-up
+    int rc = launch_stage(h, i, 1, h->cur);  // warm-up
     cudaEventRecord(e0, h->stream);
-    for (int r = 0; r < 3; ++r) launch_stage(h, L, 1, h->cur);
+    for (int r = 0; r < 3 && !rc; ++r) rc = launch_stage(h, i, 1, h->cur);
+    if (rc) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return rc;
+    }
     cudaEventRecord(e1, h->stream);
     e = cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -387,13 +469,14 @@ int build_graphs(mcv_handle *h) {
   const int ngraphs = h->mixed ? 2 : 1;
   for (int c = 0; c < ngraphs; ++c) {
     MCV_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin step capture");
-    for (int s = 0; s < num_stages(h); ++s) enqueue_stage(h, s, c);
+    int rc = MCV_OK;
+    for (int s = 0; s < num_stages(h) && !rc; ++s) rc = enqueue_stage(h, s, c);
     cudaError_t le = cudaGetLastError();
     cudaGraph_t graph = nullptr;
     cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
-    if (le != cudaSuccess) {
+    if (rc || le != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
-      return cuda_fail(le, "launch during step capture");
+      return rc ? rc : cuda_fail(le, "launch during step capture");
     }
     MCV_CUDA(ce, "end step capture");
     cudaError_t ie = cudaGraphInstantiate(&h->graph_exec[c], graph, 0);
@@ -488,6 +571,7 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   cudaDeviceProp prop;
   MCV_CUDA(cudaGetDeviceProperties(&prop, dev), "device properties");
   if (prop.major != 10) return fail(MCV_ERR_CUDA, "this library is built for sm_100a (B200) only");
+  const int nsm = prop.multiProcessorCount;
 
   mcv_handle *h = new mcv_handle();
   h->order = order; h->nc = nc; h->scheme = scheme; h->precision = precision; h->members = members;
@@ -506,11 +590,18 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->mcur.assign(members, 0);
   h->phibar_host.assign(members, 0.);
   h->cands = stage_launchers(order, h->mixed, &h->ncands);
+  h->nsm = nsm;
+  h->bps.assign(h->ncands, 0);
   for (int i = 0; i < h->ncands; ++i) {
     cudaError_t e = h->cands[i].prepare();
     if (e != cudaSuccess) {
       delete h;
       return cuda_fail(e, "set stage kernel shared memory");
+    }
+    h->bps[i] = h->cands[i].blocks_per_sm();
+    if (h->bps[i] < 1) {
+      delete h;
+      return fail(MCV_ERR_CUDA, "a stage kernel candidate cannot be resident on an SM");
     }
   }
   int rc = upload_tables();
@@ -567,6 +658,7 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->partial = (double4 *)(base + L.partial);
   h->active = (int *)(base + L.active);
   h->flags = (int *)(base + L.flags);
+  h->err = (int *)(base + L.err);
   // zero everything once: unused pitch padding and halo corners stay finite
   e = cudaMemsetAsync(h->pool, 0, L.total, h->stream);
   // every member is active until mcv_set_active says otherwise
@@ -734,6 +826,9 @@ extern "C" int mcv_step_async(mcv_handle *h, int nsteps) {
 extern "C" int mcv_sync(mcv_handle *h) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   MCV_CUDA(cudaStreamSynchronize(h->stream), "step");
+  int err = 0;
+  MCV_CUDA(cudaMemcpy(&err, h->err, sizeof(int), cudaMemcpyDeviceToHost), "read stage error flag");
+  if (err) return fail(MCV_ERR_CUDA, "stage kernel: a staged tile's copies did not arrive in time");
   return MCV_OK;
 }
 
@@ -926,7 +1021,11 @@ extern "C" int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, dou
     for (int s = 0; s < S; ++s) {
       cudaEvent_t *e = &ev[((size_t)it * S + s) * 3];
       cudaEventRecord(e[0], h->stream);
-      enqueue_stage(h, s, h->cur, e[1]);
+      if (int rc = enqueue_stage(h, s, h->cur, e[1])) {
+        cudaStreamSynchronize(h->stream);
+        for (auto &ev_ : ev) cudaEventDestroy(ev_);
+        return rc;
+      }
       cudaEventRecord(e[2], h->stream);
     }
     if (h->mixed) h->cur = 1 - h->cur;

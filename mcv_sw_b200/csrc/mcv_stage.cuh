@@ -23,6 +23,8 @@
 
 #include <type_traits>
 
+#include "mcv_tma.cuh"
+
 namespace mcv {
 
 // RK stage kinds: which combination of stage input, RK base and tendency
@@ -61,6 +63,7 @@ struct StageArgs {
   const double *phis;                               // [M][6][np][P]
   double4 *bnd;  // raw boundary copy [M][6][4][n] {u, v, phi, 0}
   double inc;    // dt or dt/2 (update_stat's inc_t) or the RK3 tendency weight
+  int *err;      // set to 1 if a staged tile's copies did not arrive in time (TMA form)
   const int *active;  // member index of each grid z slice (the members this launch advances)
   // ---- split-precision policy ----
   const double *yu, *yv, *yp;  // FP64 state Y (RK base and stage-1 input), padded; the last
@@ -247,9 +250,24 @@ struct Tile {
   // reference-point values [3][3] double, slopes [2][3] float
   static constexpr size_t MET_OFF = ((size_t)TOTAL * sizeof(R) + 31) / 32 * 32;
   static constexpr size_t PLANE_OFF = MET_OFF + (size_t)(LX + LY) * sizeof(double4);
-  static constexpr size_t bytes(bool mixed) {
+  __host__ __device__ static constexpr size_t bytes(bool mixed) {
     return mixed ? PLANE_OFF + 18 * sizeof(double) + 6 * sizeof(float) : (size_t)TOTAL * sizeof(R);
   }
+  // TMA form, after all of the above: one work item's input fields as staged
+  // boxes [LY][BX] (FP64 policy: 8 FP64 fields; split precision: 3 FP64 then 4
+  // FP32 fields), each slot 128-byte aligned, then the mbarrier
+  static constexpr int BX = (LX + 3) / 4 * 4;  // box row: a 16-byte multiple for 4- and 8-byte elements
+  static constexpr size_t FB64 = ((size_t)BX * LY * 8 + 127) / 128 * 128;
+  static constexpr size_t FB32 = ((size_t)BX * LY * 4 + 127) / 128 * 128;
+  __host__ __device__ static constexpr size_t stg_off(bool mixed) { return (bytes(mixed) + 127) / 128 * 128; }
+  __host__ __device__ static constexpr size_t field_off(bool mixed, int f) {
+    return stg_off(mixed) + (mixed ? (f < 3 ? f * FB64 : 3 * FB64 + (f - 3) * FB32) : f * FB64);
+  }
+  __host__ __device__ static constexpr uint32_t field_bytes(bool mixed, int f) {
+    return (uint32_t)BX * LY * ((mixed && f >= 3) ? 4u : 8u);
+  }
+  __host__ __device__ static constexpr size_t bar_off(bool mixed) { return field_off(mixed, mixed ? 7 : 8); }
+  __host__ __device__ static constexpr size_t bytes_tma(bool mixed) { return bar_off(mixed) + 16; }
   static_assert(LX % 2 == 1, "odd shared row length");
 };
 
@@ -283,14 +301,76 @@ __device__ __forceinline__ void mix_point(MixPoint &o, const double4 mx, const d
 }
 
 // MINB: CTAs per SM the register allocation must allow (launch bounds).
-template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, bool WALK>
-__global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const StageArgs a) {
+// TMA: persistent form -- each CTA walks work items (tile, panel, member)
+// blockIdx.x, blockIdx.x + gridDim.x, ...; the next item's input fields are
+// copied into a shared-memory staging area by TMA while the current item's
+// sweeps and update run.  Otherwise one CTA per (tile, panel, member) loads
+// its fields with ordinary loads.
+template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, bool WALK, bool TMA>
+__global__ void __launch_bounds__(NT, MINB)
+    stage_kernel(const GridDesc g, const StageArgs a, const __grid_constant__ TileMaps tm) {
   using R = std::conditional_t<MIXED, float, double>;
   using T = Tile<D, CX, CY, R>;
   constexpr int H = T::H, LX = T::LX;
-  extern __shared__ __align__(32) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
   R *sm = reinterpret_cast<R *>(smraw);
-  const int tile = blockIdx.x, panel = blockIdx.y, mem = __ldg(a.active + blockIdx.z);
+  double4 *metx = reinterpret_cast<double4 *>(smraw + T::MET_OFF);  // split precision: [LX] then [LY]
+  const double4 *mety = metx + LX;
+  double *plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF);  // [3] {value at (H, H), d/dlx, d/dly}
+  double *qref = plane + 9;                                            // [3 points][3]
+  float *slope = reinterpret_cast<float *>(qref + 9);                  // [x, y][3]: derivative per radian
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + T::bar_off(MIXED));
+  const int ntile = g.tiles_x * g.tiles_y;
+  // number of staged fields (split precision: the first stage has no input increment)
+  constexpr int NF = MIXED ? (first_stage(KIND) ? 4 : 7) : 8;
+
+  // TMA: issue the copies of work item wi's input fields (one thread)
+  auto issue = [&](int wi) {
+    const int tile = wi % ntile, rest = wi / ntile;
+    const int panel = rest % 6, mem = __ldg(a.active + rest / 6);
+    const int X0 = (tile % g.tiles_x) * CX * (D - 1), Y0 = (tile / g.tiles_x) * CY * (D - 1);
+    uint32_t bytes = 0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) bytes += T::field_bytes(MIXED, f);
+    int nx = 0, ny = 0;
+    if constexpr (MIXED) {
+      nx = min(LX, g.np - X0);
+      ny = min(T::LY, g.np - Y0);
+      bytes += (uint32_t)(nx + ny) * sizeof(double4);
+    }
+    mbar_arrive_expect_tx(bar, bytes);
+    const int srow = (mem * 6 + panel) * g.np + Y0;  // row of a per-member field
+    const int mrow = panel * g.np + Y0;              // row of a metric plane
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+      tma_load_2d(smraw + T::field_off(MIXED, f), &tm.f[f], X0, (!MIXED && f >= 4) ? mrow : srow, bar);
+    if constexpr (MIXED) {
+      bulk_load(metx, a.met1d + X0, (uint32_t)nx * sizeof(double4), bar);
+      bulk_load(metx + LX, a.met1d + Y0, (uint32_t)ny * sizeof(double4), bar);
+    }
+  };
+  uint32_t parity = 0;
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && (int)blockIdx.x < tm.total) issue(blockIdx.x);
+  }
+  const int wfirst = TMA ? (int)blockIdx.x : 0, wstep = TMA ? (int)gridDim.x : 1, wend = TMA ? tm.total : 1;
+  for (int wi = wfirst; wi < wend; wi += wstep) {
+  int tile, panel, mem;
+  if constexpr (TMA) {
+    tile = wi % ntile;
+    const int rest = wi / ntile;
+    panel = rest % 6;
+    mem = __ldg(a.active + rest / 6);
+  } else {
+    tile = blockIdx.x;
+    panel = blockIdx.y;
+    mem = __ldg(a.active + blockIdx.z);
+  }
   const int tx = tile % g.tiles_x, ty = tile / g.tiles_x;
   const int c0x = tx * CX, c0y = ty * CY;
   const int ncx = min(CX, g.Nc - c0x), ncy = min(CY, g.Nc - c0y);
@@ -300,11 +380,6 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const
   const long long mbase = (long long)mem * g.mstride + pbase;
   const int txe = ncx * (D - 1) + 1, tye = ncy * (D - 1) + 1;  // tile points per row / column
   const double phibar = MIXED ? a.phibar[mem] : 0.;
-  double4 *metx = reinterpret_cast<double4 *>(smraw + T::MET_OFF);  // split precision: [LX] then [LY]
-  const double4 *mety = metx + LX;
-  double *plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF);  // [3] {value at (H, H), d/dlx, d/dly}
-  double *qref = plane + 9;                                            // [3 points][3]
-  float *slope = reinterpret_cast<float *>(qref + 9);                  // [x, y][3]: derivative per radian
 
   // ---- phase 0: load the tile and its halo cross, pointwise quantities ----
   // (spatial_operators_mod.F90:58-61, eigenvalues :248-280, upwind signs :83-85)
@@ -327,7 +402,162 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const
   const double *t_yu = a.yu + mbase + tbase, *t_yv = a.yv + mbase + tbase, *t_yp = a.yp + mbase + tbase;
   const float *t_du = a.du + mbase + tbase, *t_dv = a.dv + mbase + tbase, *t_dp = a.dp + mbase + tbase;
   const float *t_p32 = a.phis32 + mbase + tbase;
-  {
+
+  // staged field f at loaded point (lx, ly) (TMA form)
+  auto stg64 = [&](int f, int lx, int ly) {
+    return reinterpret_cast<const double *>(smraw + T::field_off(MIXED, f))[ly * T::BX + lx];
+  };
+  auto stg32 = [&](int f, int lx, int ly) {
+    return reinterpret_cast<const float *>(smraw + T::field_off(MIXED, f))[ly * T::BX + lx];
+  };
+
+  // split precision: the per-tile linear references (two block barriers)
+  auto make_planes = [&]() {
+    if (threadIdx.x < 3) {
+      // reference points (H, H), (txe - 1 + H, H), (H, tye - 1 + H): interior
+      const int lx = H + (threadIdx.x == 1 ? txe - 1 : 0), ly = H + (threadIdx.x == 2 ? tye - 1 : 0);
+      double u, v, p, phs;
+      if constexpr (TMA) {
+        u = stg64(0, lx, ly);
+        v = stg64(1, lx, ly);
+        p = stg64(2, lx, ly);
+        phs = (double)stg32(3, lx, ly);
+        if constexpr (!first_stage(KIND)) {
+          u += (double)stg32(4, lx, ly);
+          v += (double)stg32(5, lx, ly);
+          p += (double)stg32(6, lx, ly);
+        }
+      } else {
+        const int o = ly * g.P + lx;
+        u = __ldg(t_yu + o);
+        v = __ldg(t_yv + o);
+        p = __ldg(t_yp + o);
+        phs = (double)__ldg(t_p32 + o);
+        if constexpr (!first_stage(KIND)) {
+          u += (double)__ldg(t_du + o);
+          v += (double)__ldg(t_dv + o);
+          p += (double)__ldg(t_dp + o);
+        }
+      }
+      MixPoint mp;
+      mix_point(mp, a.met1d[X0 + lx], a.met1d[Y0 + ly], u, v, p, phs, phibar, panel, a.two_omega);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) qref[threadIdx.x * 3 + q] = mp.q[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      // The derivative added back is FP32, so the plane takes its slope from
+      // the rounded value: the two agree to FP64 rounding.
+      const int q = threadIdx.x;
+      const double q0 = qref[q];
+      const float sx = (float)((qref[3 + q] - q0) / ((double)ncx * g.dx));
+      const float sy = (float)((qref[6 + q] - q0) / ((double)ncy * g.dx));
+      plane[3 * q] = q0;
+      plane[3 * q + 1] = (double)sx * (g.dx / (double)(D - 1));  // per point index
+      plane[3 * q + 2] = (double)sy * (g.dx / (double)(D - 1));
+      slope[q] = sx;
+      slope[3 + q] = sy;
+    }
+    __syncthreads();
+  };
+
+  // one loaded point: r = {u, v, phi, phi_s, sqrtG, G^11, G^12, G^22} (FP64
+  // policy) or {Y_u, Y_v, Y_phi} with f = {phi_s, d_u, d_v, d_phi} (split)
+  auto point = [&](int idx, int lx, int ly, const double *r, const float *f) {
+    R u, v, phi, sg, g11, g22, cu, cv, fc = R(0);
+    if constexpr (!MIXED) {
+      u = r[0]; v = r[1]; phi = r[2];
+      const double phs = r[3];
+      sg = r[4]; g11 = r[5];
+      const double g12 = r[6];
+      g22 = r[7];
+      const double pg = phi * sg;
+      cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
+      cv = g12 * u + g22 * v;
+      sm[T::U + idx] = u;
+      sm[T::V + idx] = v;
+      sm[T::PG + idx] = pg;
+      sm[T::PGU + idx] = pg * cu;
+      sm[T::PGV + idx] = pg * cv;
+      sm[T::E + idx] = phi + phs + 0.5 * (cu * u + cv * v);  // E = phi + phi_s + K
+    } else {
+      double u64 = r[0], v64 = r[1], p64 = r[2];
+      if constexpr (!first_stage(KIND)) {
+        u64 += (double)f[1];
+        v64 += (double)f[2];
+        p64 += (double)f[3];
+      }
+      MixPoint mp;
+      mix_point(mp, metx[lx], mety[ly], u64, v64, p64, (double)f[0], phibar, panel, a.two_omega);
+      const double X = (double)(lx - H), Y = (double)(ly - H);
+      sm[T::E + idx] = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
+      sm[T::U + idx] = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
+      sm[T::V + idx] = (float)(mp.q[2] - (plane[6] + plane[7] * X + plane[8] * Y));
+      sm[T::PG + idx] = (float)mp.q[3];
+      sm[T::PGU + idx] = (float)mp.q[4];
+      sm[T::PGV + idx] = (float)mp.q[5];
+      u = (R)u64;
+      v = (R)v64;
+      phi = (R)p64;
+      sg = (R)mp.sg;
+      g11 = (R)mp.g11;
+      g22 = (R)mp.g22;
+      cu = (R)mp.cu;
+      cv = (R)mp.cv;
+      fc = (R)mp.fc;
+    }
+    const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
+    if (!xh && !yh) {
+      const int ix = lx - H, iy = ly - H;
+      const int ii = iy * T::TX + ix;
+      sm[T::SG + ii] = sg;
+      sm[T::CU + ii] = cu;
+      sm[T::CV + ii] = cv;
+      if constexpr (MIXED) sm[T::FC + ii] = fc;
+      // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
+      if (ix % (D - 1) == 0) {
+        sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
+        sm[T::SGNX + iy * (CX + 1) + ix / (D - 1)] = (cu < R(0)) ? R(-1) : R(1);
+      }
+      if (iy % (D - 1) == 0) {
+        sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
+        sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < R(0)) ? R(-1) : R(1);
+      }
+    }
+  };
+
+  if constexpr (TMA) {
+    // wait for this item's copies; every thread agrees before anyone leaves
+    const bool ok = mbar_wait_bounded(bar, parity);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicExch(a.err, 1);
+      mbar_wait_bounded(bar, parity);  // the copies in flight land before the CTA exits
+      return;
+    }
+    parity ^= 1u;
+    if constexpr (MIXED) make_planes();
+    for (int idx = threadIdx.x; idx < T::A; idx += NT) {
+      const int ly = idx / LX, lx = idx - ly * LX;
+      const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
+      if (lx >= lxe || ly >= lye || (xh && yh)) continue;  // tile corners are never read
+      double r[8];
+      float f[4];
+      if constexpr (!MIXED) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) r[k] = stg64(k, lx, ly);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) r[k] = stg64(k, lx, ly);
+        f[0] = stg32(3, lx, ly);
+        if constexpr (!first_stage(KIND)) {
+          f[1] = stg32(4, lx, ly);
+          f[2] = stg32(5, lx, ly);
+          f[3] = stg32(6, lx, ly);
+        }
+      }
+      point(idx, lx, ly, r, f);
+    }
+  } else {
     constexpr int CH = 3;  // points per thread whose loads are in flight together
     constexpr int NL = MIXED ? 3 : 8;
     for (int base = 0; base < T::A; base += NT * CH) {
@@ -371,37 +601,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const
             const int gidx = (k < LX) ? X0 + k : Y0 + (k - LX);
             if (gidx < g.np) metx[k] = a.met1d[gidx];
           }
-          if (threadIdx.x < 3) {
-            // reference points (H, H), (txe - 1 + H, H), (H, tye - 1 + H): interior
-            const int lx = H + (threadIdx.x == 1 ? txe - 1 : 0), ly = H + (threadIdx.x == 2 ? tye - 1 : 0);
-            const int o = ly * g.P + lx;
-            double u = __ldg(t_yu + o), v = __ldg(t_yv + o), p = __ldg(t_yp + o);
-            if constexpr (!first_stage(KIND)) {
-              u += (double)__ldg(t_du + o);
-              v += (double)__ldg(t_dv + o);
-              p += (double)__ldg(t_dp + o);
-            }
-            MixPoint mp;
-            mix_point(mp, a.met1d[X0 + lx], a.met1d[Y0 + ly], u, v, p, (double)__ldg(t_p32 + o), phibar, panel,
-                      a.two_omega);
-#pragma unroll
-            for (int q = 0; q < 3; ++q) qref[threadIdx.x * 3 + q] = mp.q[q];
-          }
-          __syncthreads();
-          if (threadIdx.x < 3) {
-            // The derivative added back is FP32, so the plane takes its slope
-            // from the rounded value: the two agree to FP64 rounding.
-            const int q = threadIdx.x;
-            const double q0 = qref[q];
-            const float sx = (float)((qref[3 + q] - q0) / ((double)ncx * g.dx));
-            const float sy = (float)((qref[6 + q] - q0) / ((double)ncy * g.dx));
-            plane[3 * q] = q0;
-            plane[3 * q + 1] = (double)sx * (g.dx / (double)(D - 1));  // per point index
-            plane[3 * q + 2] = (double)sy * (g.dx / (double)(D - 1));
-            slope[q] = sx;
-            slope[3 + q] = sy;
-          }
-          __syncthreads();
+          make_planes();
         }
       }
 #pragma unroll
@@ -409,70 +609,24 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const
         if (!ok[k]) continue;
         const int idx = base + threadIdx.x + k * NT;
         const int ly = idx / LX, lx = idx - ly * LX;
-        R u, v, phi, sg, g11, g22, cu, cv, fc = R(0);
-        if constexpr (!MIXED) {
-          u = r[0][k]; v = r[1][k]; phi = r[2][k];
-          const double phs = r[3][k];
-          sg = r[4][k]; g11 = r[5][k];
-          const double g12 = r[6][k];
-          g22 = r[7][k];
-          const double pg = phi * sg;
-          cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
-          cv = g12 * u + g22 * v;
-          sm[T::U + idx] = u;
-          sm[T::V + idx] = v;
-          sm[T::PG + idx] = pg;
-          sm[T::PGU + idx] = pg * cu;
-          sm[T::PGV + idx] = pg * cv;
-          sm[T::E + idx] = phi + phs + 0.5 * (cu * u + cv * v);  // E = phi + phi_s + K
-        } else {
-          double u64 = r[0][k], v64 = r[1][k], p64 = r[2][k];
-          if constexpr (!first_stage(KIND)) {
-            u64 += (double)f[1][k];
-            v64 += (double)f[2][k];
-            p64 += (double)f[3][k];
-          }
-          MixPoint mp;
-          mix_point(mp, metx[lx], mety[ly], u64, v64, p64, (double)f[0][k], phibar, panel, a.two_omega);
-          const double X = (double)(lx - H), Y = (double)(ly - H);
-          sm[T::E + idx] = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
-          sm[T::U + idx] = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
-          sm[T::V + idx] = (float)(mp.q[2] - (plane[6] + plane[7] * X + plane[8] * Y));
-          sm[T::PG + idx] = (float)mp.q[3];
-          sm[T::PGU + idx] = (float)mp.q[4];
-          sm[T::PGV + idx] = (float)mp.q[5];
-          u = (R)u64;
-          v = (R)v64;
-          phi = (R)p64;
-          sg = (R)mp.sg;
-          g11 = (R)mp.g11;
-          g22 = (R)mp.g22;
-          cu = (R)mp.cu;
-          cv = (R)mp.cv;
-          fc = (R)mp.fc;
-        }
-        const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
-        if (!xh && !yh) {
-          const int ix = lx - H, iy = ly - H;
-          const int ii = iy * T::TX + ix;
-          sm[T::SG + ii] = sg;
-          sm[T::CU + ii] = cu;
-          sm[T::CV + ii] = cv;
-          if constexpr (MIXED) sm[T::FC + ii] = fc;
-          // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
-          if (ix % (D - 1) == 0) {
-            sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
-            sm[T::SGNX + iy * (CX + 1) + ix / (D - 1)] = (cu < R(0)) ? R(-1) : R(1);
-          }
-          if (iy % (D - 1) == 0) {
-            sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
-            sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < R(0)) ? R(-1) : R(1);
-          }
-        }
+        double rr[8];
+        float ff[4];
+#pragma unroll
+        for (int j = 0; j < NL; ++j) rr[j] = r[j][k];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) ff[j] = f[j][k];
+        point(idx, lx, ly, rr, ff);
       }
     }
   }
   __syncthreads();
+  if constexpr (TMA) {
+    // the staging area is free: start the copies of this CTA's next item
+    if (threadIdx.x == 0 && wi + wstep < wend) {
+      fence_proxy_async();
+      issue(wi + wstep);
+    }
+  }
   const Widths<R> w(g);
 
   if constexpr (!WALK) {
@@ -681,37 +835,44 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const GridDesc g, const
       }
     }
   }
+  if constexpr (TMA) __syncthreads();  // the next item reuses the shared arrays
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Launch table of one tile shape (used by the tile-shape autotuner).
 // ---------------------------------------------------------------------------
-using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a);
+using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a,
+                               const TileMaps &tm);
 
 struct StageLauncher {
   int CX, CY, NT, minb;
   bool walk;  // sweeps as line walks instead of per-cell items
+  bool tma;   // persistent CTAs with TMA-staged tiles
   size_t smem;
+  int box_x, box_y;         // staged box of one field (TMA form)
   StageLaunchFn launch[7];  // indexed by StageKind
-  cudaError_t (*prepare)(); // shared-memory limit and carveout of every kind
+  cudaError_t (*prepare)(); // raises the dynamic shared-memory limit of every kind
+  int (*blocks_per_sm)();   // resident CTAs per SM (sizes the persistent grid)
 };
 
-template <int D, int CX, int CY, int NT, int MINB, bool MIXED, bool WALK>
+template <int D, int CX, int CY, int NT, int MINB, bool MIXED, bool WALK, bool TMA = false>
 struct StageConfig {
   using T = Tile<D, CX, CY, std::conditional_t<MIXED, float, double>>;
-  static constexpr size_t SMEM = T::bytes(MIXED);
+  static constexpr size_t SMEM = TMA ? T::bytes_tma(MIXED) : T::bytes(MIXED);
+  // TMA box x coordinates are tile origins X0 = tile * CX * (D - 1): their byte
+  // offsets must be multiples of 16 (FP32 fields: X0 % 4 == 0; FP64: even)
+  static_assert(!TMA || (CX * (D - 1)) % (MIXED ? 4 : 2) == 0, "TMA box origin not 16-byte aligned");
   template <int KIND>
-  static void launch(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a) {
-    stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK><<<grid, NT, SMEM, s>>>(g, a);
+  static void launch(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a, const TileMaps &tm) {
+    stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA><<<grid, NT, SMEM, s>>>(g, a, tm);
   }
   template <int KIND>
   static cudaError_t attr() {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    if (e != cudaSuccess) return e;
-    // the largest shared-memory carveout, so that MINB tiles fit on an SM
-    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK>,
-                                cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    // (the driver's own carveout choice: forcing the largest shared-memory
+    // carveout shrank L1 and slowed the FP64 kernels by up to 20%)
+    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
   static cudaError_t prepare() {
     cudaError_t e;
@@ -720,12 +881,19 @@ struct StageConfig {
       return e;
     return cudaSuccess;
   }
+  static int blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA>, NT,
+                                                      SMEM) != cudaSuccess)
+      return 0;
+    return n;
+  }
   static StageLauncher make() {
     static_assert(SMEM <= 227 * 1024, "tile does not fit in shared memory");
     static_assert(MINB * (SMEM + 1024) <= 228 * 1024, "MINB tiles do not fit in one SM's shared memory");
-    return StageLauncher{CX, CY, NT, MINB, WALK, SMEM,
+    return StageLauncher{CX,     CY,    NT,    MINB,  WALK, TMA, SMEM, T::BX, T::LY,
                          {&launch<0>, &launch<1>, &launch<2>, &launch<3>, &launch<4>, &launch<5>, &launch<6>},
-                         &prepare};
+                         &prepare, &blocks_per_sm};
   }
 };
 

@@ -1,6 +1,6 @@
 // stage_d3_f64.cu -- stage-kernel instantiations for MCV3, FP64:
 // the tile shapes (cells x cells, threads, CTAs per SM the registers must allow,
-// sweep style) the autotuner chooses from.
+// sweep style, TMA-staged persistent form) the autotuner chooses from.
 #include "mcv_stage.cuh"
 
 namespace mcv {
@@ -11,7 +11,8 @@ const StageLauncher *stage_launchers_d3_f64(int *count) {
     StageConfig<3, 8, 8, 224, 4, false, false>::make(),
     StageConfig<3, 8, 8, 160, 4, false, false>::make(),
     StageConfig<3, 16, 8, 384, 2, false, false>::make(),
-    StageConfig<3, 12, 12, 160, 2, false, true>::make()};
+    StageConfig<3, 12, 12, 160, 2, false, true>::make(),
+    StageConfig<3, 8, 8, 224, 2, false, false, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }

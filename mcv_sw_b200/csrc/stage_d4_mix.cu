@@ -1,6 +1,6 @@
 // stage_d4_mix.cu -- stage-kernel instantiations for MCV4, split precision:
 // the tile shapes (cells x cells, threads, CTAs per SM the registers must allow,
-// sweep style) the autotuner chooses from.
+// sweep style, TMA-staged persistent form) the autotuner chooses from.
 #include "mcv_stage.cuh"
 
 namespace mcv {
@@ -11,7 +11,9 @@ const StageLauncher *stage_launchers_d4_mix(int *count) {
     StageConfig<4, 8, 8, 320, 3, true, false>::make(),
     StageConfig<4, 8, 8, 256, 4, true, false>::make(),
     StageConfig<4, 8, 8, 384, 2, true, false>::make(),
-    StageConfig<4, 12, 12, 224, 1, true, true>::make()};
+    StageConfig<4, 12, 12, 224, 1, true, true>::make(),
+    StageConfig<4, 8, 8, 256, 2, true, false, true>::make(),
+    StageConfig<4, 8, 8, 320, 2, true, false, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }
