@@ -47,6 +47,9 @@ def parse_args():
     p.add_argument("--ensemble", type=int, default=1, help="run the 64-member ensemble block (1 GPU only)")
     p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving block (0: skip)")
     p.add_argument("--stress", type=int, default=1, help="run the Nc=1024 roofline-stress block (1 GPU only)")
+    p.add_argument("--tiles", default=None,
+                   help="pin the stage-kernel candidates of the main workload as 'fp64_index,mixed_index' "
+                        "(default: each handle's autotuner chooses)")
     return p.parse_args()
 
 
@@ -212,6 +215,8 @@ def time_path(args, st, geom, precision, world, barrier, dist, local):
     n_pv = 6 * geom.n * geom.n
     s = api.Stepper(st.order, st.nc, st.dt, st.scheme, members=1, precision=precision, radius=6.371e6)
     s.set_geometry(geom)
+    if args.tiles:
+        s.select_tile(int(args.tiles.split(",")[0 if precision == "fp64" else 1]))
     s.set_member(0, st.phi_s, st.u, st.v, st.phi)
     s.time_steps(max(args.warmup, 3))
     barrier()

@@ -65,13 +65,17 @@ def harmonic_height(geom, rng, lmin, lmax, rms):
 
 
 def cfl_dt(geom, u, v, phi, cfl=0.5):
-    """dt = cfl * (dx/(D-1)) / max over interior PVs of |c^i| + sqrt(G^ii phi)."""
+    """dt = cfl * (dx/(D-1)) / max over interior PVs of the two directions'
+    signal speeds summed, (|c^1| + sqrt(G^11 phi)) + (|c^2| + sqrt(G^22 phi)):
+    the CFL number of a dimension-split explicit scheme in two dimensions.
+    (With the larger of the two speeds instead of their sum, dt is ~1.8x
+    longer and RK4 runs of jets crossing the cube's corners blow up in FP64.)"""
     IG = geom.matrixIG
     cu = IG[..., 0, 0] * u + IG[..., 1, 0] * v
     cv = IG[..., 0, 1] * u + IG[..., 1, 1] * v
     sx = np.abs(cu) + np.sqrt(IG[..., 0, 0] * phi)
     sy = np.abs(cv) + np.sqrt(IG[..., 1, 1] * phi)
-    smax = max(float(geom.interior(sx).max()), float(geom.interior(sy).max()))
+    smax = float(geom.interior(sx + sy).max())
     return cfl * (geom.dx / (geom.order - 1)) / smax
 
 

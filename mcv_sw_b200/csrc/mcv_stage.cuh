@@ -140,6 +140,82 @@ __device__ __forceinline__ void cell_derivs(R out[D], const R *f, const R *q, R 
   }
 }
 
+// Split precision: calc_tendP for two quantities at once, one in each half of
+// a float2 (packed FP32 FMA, FFMA2); both use the same eigenvalues.  Same
+// formulas as cell_derivs, with the sums ordered explicitly.
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+template <int D>
+__device__ __forceinline__ float2 polyfit_left2(const float2 *p, float2 inv) {
+  if constexpr (D == 3) {
+    // -(p2 - 4 p1 + 3 p0) / dh
+    const float2 t = fma2(bc2(3.f), p[0], fma2(bc2(-4.f), p[1], p[2]));
+    return mul2(t, make_float2(-inv.x, -inv.y));
+  } else {
+    // (-11 p0 + 18 p1 - 9 p2 + 2 p3) / (2 dh)
+    float2 t = mul2(bc2(2.f), p[3]);
+    t = fma2(bc2(-9.f), p[2], t);
+    t = fma2(bc2(18.f), p[1], t);
+    t = fma2(bc2(-11.f), p[0], t);
+    return mul2(t, inv);
+  }
+}
+template <int D>
+__device__ __forceinline__ float2 polyfit_right2(const float2 *p, float2 inv) {
+  if constexpr (D == 3) {
+    // (p0 - 4 p1 + 3 p2) / dh
+    const float2 t = fma2(bc2(3.f), p[2], fma2(bc2(-4.f), p[1], p[0]));
+    return mul2(t, inv);
+  } else {
+    // (11 p3 - 18 p2 + 9 p1 - 2 p0) / (2 dh)
+    float2 t = mul2(bc2(-2.f), p[0]);
+    t = fma2(bc2(9.f), p[1], t);
+    t = fma2(bc2(-18.f), p[2], t);
+    t = fma2(bc2(11.f), p[3], t);
+    return mul2(t, inv);
+  }
+}
+__device__ __forceinline__ float2 riemann2(float2 fL, float2 fR, float2 qL, float2 qR, float lam) {
+  const float2 dq = fma2(bc2(-1.f), qL, qR);
+  return mul2(bc2(0.5f), fma2(bc2(-lam), dq, add2(fL, fR)));
+}
+
+template <int D, int S>
+__device__ __forceinline__ void cell_derivs2(float2 out[D], const float2 *f, const float2 *q, float lamL, float lamR,
+                                             const Widths<float> &w) {
+  const float ipf = (D == 3) ? w.inv_dx : w.inv_2dx;
+  const float2 ip = bc2(ipf);
+  float2 c1[D], c2[D], c3[D], d1[D], d2[D], d3[D];
+#pragma unroll
+  for (int m = 0; m < D; ++m) {
+    c1[m] = f[m * S];
+    c2[m] = f[(D - 1 + m) * S];
+    c3[m] = f[(2 * D - 2 + m) * S];
+    d1[m] = q[m * S];
+    d2[m] = q[(D - 1 + m) * S];
+    d3[m] = q[(2 * D - 2 + m) * S];
+  }
+  out[0] = riemann2(polyfit_right2<D>(c1, ip), polyfit_left2<D>(c2, ip), polyfit_right2<D>(d1, ip),
+                    polyfit_left2<D>(d2, ip), lamL);
+  out[D - 1] = riemann2(polyfit_right2<D>(c2, ip), polyfit_left2<D>(c3, ip), polyfit_right2<D>(d2, ip),
+                        polyfit_left2<D>(d3, ip), lamR);
+  const float2 via = mul2(fma2(bc2(-1.f), c2[0], c2[D - 1]), bc2(w.inv_dx));  // (f_R - f_L)/dx
+  if constexpr (D == 3) {
+    out[1] = fma2(bc2(1.5f), via, mul2(bc2(-0.25f), add2(out[0], out[2])));
+  } else {
+    // 4/27 dx * 4.5 (c0 - c1 - c2 + c3)/dx^2 = (2/3)(c0 - c1 - c2 + c3)/dx
+    const float2 t = fma2(bc2(-1.f), c2[2], fma2(bc2(-1.f), c2[1], add2(c2[0], c2[3])));
+    const float2 k = mul2(bc2(2.f / 3.f), mul2(t, bc2(w.inv_dx)));
+    float2 a = fma2(bc2(-4.f / 27.f), out[0], mul2(bc2(4.f / 3.f), via));
+    out[1] = fma2(bc2(-1.f), k, fma2(bc2(-5.f / 27.f), out[3], a));
+    a = fma2(bc2(-5.f / 27.f), out[0], mul2(bc2(4.f / 3.f), via));
+    out[2] = add2(k, fma2(bc2(-4.f / 27.f), out[3], a));
+  }
+}
+
 // calc_tendP (src/spatial_operators_mod.F90:136-202) applied to every cell of
 // one grid line of `ncells` cells, as the x-sweep (:63-93) and y-sweep (:95-125)
 // do for each row and column.  f and q point to the first point of the halo
@@ -232,10 +308,15 @@ struct Tile {
   static constexpr int LY = TY + 2 * H;
   static constexpr int A = LX * LY;  // loaded rectangle (corners unused)
   static constexpr int I = TX * TY;  // tile interior
-  // shared-memory carve (elements of R): full-rectangle arrays ...
+  // shared-memory carve (elements of R): full-rectangle arrays -- FP64 policy:
+  // u, v, E, phiG, phiG cU, phiG cV; split precision: u, v and the sweep pairs
+  // as float2 [A] each: XF = (E, phiG cU), XQ = (u, phiG), YF = (E, phiG cV),
+  // YQ = (v, phiG) (the x and y sweeps' flux and Riemann fields) ...
+  static constexpr bool PAIRED = std::is_same<R, float>::value;
   static constexpr int U = 0, V = A, E = 2 * A, PG = 3 * A, PGU = 4 * A, PGV = 5 * A;
+  static constexpr int XF = 2 * A, XQ = 4 * A, YF = 6 * A, YQ = 8 * A;  // in floats (even: float2-aligned)
   // ... interior-only arrays ...
-  static constexpr int SG = 6 * A, CU = SG + I, CV = CU + I, FC = CV + I;
+  static constexpr int SG = (PAIRED ? 10 : 6) * A, CU = SG + I, CV = CU + I, FC = CV + I;
   // ... interface eigenvalues and upwind signs ...
   static constexpr int LAMX = FC + I;                // [TY][CX+1]
   static constexpr int SGNX = LAMX + TY * (CX + 1);
@@ -464,50 +545,9 @@ __global__ void __launch_bounds__(NT, MINB)
   // one loaded point: r = {u, v, phi, phi_s, sqrtG, G^11, G^12, G^22} (FP64
   // policy) or {Y_u, Y_v, Y_phi} with f = {phi_s, d_u, d_v, d_phi} (split)
   auto point = [&](int idx, int lx, int ly, const double *r, const float *f) {
-    R u, v, phi, sg, g11, g22, cu, cv, fc = R(0);
-    if constexpr (!MIXED) {
-      u = r[0]; v = r[1]; phi = r[2];
-      const double phs = r[3];
-      sg = r[4]; g11 = r[5];
-      const double g12 = r[6];
-      g22 = r[7];
-      const double pg = phi * sg;
-      cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
-      cv = g12 * u + g22 * v;
-      sm[T::U + idx] = u;
-      sm[T::V + idx] = v;
-      sm[T::PG + idx] = pg;
-      sm[T::PGU + idx] = pg * cu;
-      sm[T::PGV + idx] = pg * cv;
-      sm[T::E + idx] = phi + phs + 0.5 * (cu * u + cv * v);  // E = phi + phi_s + K
-    } else {
-      double u64 = r[0], v64 = r[1], p64 = r[2];
-      if constexpr (!first_stage(KIND)) {
-        u64 += (double)f[1];
-        v64 += (double)f[2];
-        p64 += (double)f[3];
-      }
-      MixPoint mp;
-      mix_point(mp, metx[lx], mety[ly], u64, v64, p64, (double)f[0], phibar, panel, a.two_omega);
-      const double X = (double)(lx - H), Y = (double)(ly - H);
-      sm[T::E + idx] = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
-      sm[T::U + idx] = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
-      sm[T::V + idx] = (float)(mp.q[2] - (plane[6] + plane[7] * X + plane[8] * Y));
-      sm[T::PG + idx] = (float)mp.q[3];
-      sm[T::PGU + idx] = (float)mp.q[4];
-      sm[T::PGV + idx] = (float)mp.q[5];
-      u = (R)u64;
-      v = (R)v64;
-      phi = (R)p64;
-      sg = (R)mp.sg;
-      g11 = (R)mp.g11;
-      g22 = (R)mp.g22;
-      cu = (R)mp.cu;
-      cv = (R)mp.cv;
-      fc = (R)mp.fc;
-    }
-    const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
-    if (!xh && !yh) {
+    // interior points also keep sqrtG, cU, cV (and f) and form the interface
+    // eigenvalues and upwind signs; split precision rounds those to FP32 here
+    auto interior = [&](R sg, R cu, R cv, R fc, R g11, R g22, R phi) {
       const int ix = lx - H, iy = ly - H;
       const int ii = iy * T::TX + ix;
       sm[T::SG + ii] = sg;
@@ -523,6 +563,44 @@ __global__ void __launch_bounds__(NT, MINB)
         sm[T::LAMY + ix * (CY + 1) + iy / (D - 1)] = fabs(cv) + sqrt(g22 * phi);
         sm[T::SGNY + ix * (CY + 1) + iy / (D - 1)] = (cv < R(0)) ? R(-1) : R(1);
       }
+    };
+    const bool inner = !((lx < H) || (lx >= lxe - H) || (ly < H) || (ly >= lye - H));
+    if constexpr (!MIXED) {
+      const double u = r[0], v = r[1], phi = r[2], phs = r[3], sg = r[4];
+      const double g11 = r[5], g12 = r[6], g22 = r[7];
+      const double pg = phi * sg;
+      const double cu = g11 * u + g12 * v;  // cov2contrav, projection_mod.F90:138-148
+      const double cv = g12 * u + g22 * v;
+      sm[T::U + idx] = u;
+      sm[T::V + idx] = v;
+      sm[T::PG + idx] = pg;
+      sm[T::PGU + idx] = pg * cu;
+      sm[T::PGV + idx] = pg * cv;
+      sm[T::E + idx] = phi + phs + 0.5 * (cu * u + cv * v);  // E = phi + phi_s + K
+      if (inner) interior(sg, cu, cv, 0., g11, g22, phi);
+    } else {
+      double u64 = r[0], v64 = r[1], p64 = r[2];
+      if constexpr (!first_stage(KIND)) {
+        u64 += (double)f[1];
+        v64 += (double)f[2];
+        p64 += (double)f[3];
+      }
+      MixPoint mp;
+      mix_point(mp, metx[lx], mety[ly], u64, v64, p64, (double)f[0], phibar, panel, a.two_omega);
+      const double X = (double)(lx - H), Y = (double)(ly - H);
+      const float e = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
+      const float uu = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
+      const float vv = (float)(mp.q[2] - (plane[6] + plane[7] * X + plane[8] * Y));
+      const float pg = (float)mp.q[3];
+      float2 *s2 = reinterpret_cast<float2 *>(sm);
+      sm[T::U + idx] = uu;
+      sm[T::V + idx] = vv;
+      s2[T::XF / 2 + idx] = make_float2(e, (float)mp.q[4]);
+      s2[T::XQ / 2 + idx] = make_float2(uu, pg);
+      s2[T::YF / 2 + idx] = make_float2(e, (float)mp.q[5]);
+      s2[T::YQ / 2 + idx] = make_float2(vv, pg);
+      if (inner)
+        interior((float)mp.sg, (float)mp.cu, (float)mp.cv, (float)mp.fc, (float)mp.g11, (float)mp.g22, (float)p64);
     }
   };
 
@@ -629,7 +707,68 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   const Widths<R> w(g);
 
-  if constexpr (!WALK) {
+  if constexpr (MIXED) {
+    static_assert(!WALK, "split precision sweeps are per-cell items");
+    // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), item = (row, cell, kind) ----
+    // kind 0: flux_x = d(E)/dx (Riemann on u) and div_x = d(phiG cU)/dx (Riemann
+    // on phiG) as one float2 pair; kind 1: dvdx, upwinded by sign(cU)
+    const float2 *s2 = reinterpret_cast<const float2 *>(sm);
+    for (int it = threadIdx.x; it < T::TY * CX * 2; it += NT) {
+      const int r = it % T::TY, rest = it / T::TY;
+      const int c = rest % CX, kk = rest / CX;
+      if (r >= tye || c >= ncx) continue;
+      const int w0 = (r + H) * LX + c * (D - 1);
+      const int mmax = (c == ncx - 1) ? D : D - 1;
+      R *xr = sm + T::XR + r * T::TX + c * (D - 1);
+      if (kk == 0) {
+        float2 d[D];
+        cell_derivs2<D, 1>(d, s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, sm[T::LAMX + r * (CX + 1) + c],
+                           sm[T::LAMX + r * (CX + 1) + c + 1], w);
+#pragma unroll
+        for (int m = 0; m < D; ++m)
+          if (m < mmax) {
+            xr[m] = d[m].x;
+            xr[T::I + m] = d[m].y;
+          }
+      } else {
+        R d[D];
+        cell_derivs<D, 1, R>(d, sm + T::V + w0, sm + T::V + w0, sm[T::SGNX + r * (CX + 1) + c],
+                             sm[T::SGNX + r * (CX + 1) + c + 1], w);
+#pragma unroll
+        for (int m = 0; m < D; ++m)
+          if (m < mmax) xr[2 * T::I + m] = d[m];
+      }
+    }
+    // ---- phase Y: y-sweep (:95-125), item = (column, cell, kind) ----
+    // kind 0: flux_y = d(E)/dy (Riemann on v) and div_y = d(phiG cV)/dy; kind 1: dudy
+    for (int it = threadIdx.x; it < T::TX * CY * 2; it += NT) {
+      const int q = it % T::TX, rest = it / T::TX;
+      const int c = rest % CY, kk = rest / CY;
+      if (q >= txe || c >= ncy) continue;
+      const int w0 = (c * (D - 1)) * LX + (q + H);
+      const int mmax = (c == ncy - 1) ? D : D - 1;
+      R *yr = sm + T::YR + (c * (D - 1)) * T::TX + q;
+      if (kk == 0) {
+        float2 d[D];
+        cell_derivs2<D, LX>(d, s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, sm[T::LAMY + q * (CY + 1) + c],
+                            sm[T::LAMY + q * (CY + 1) + c + 1], w);
+#pragma unroll
+        for (int m = 0; m < D; ++m)
+          if (m < mmax) {
+            yr[m * T::TX] = d[m].x;
+            yr[T::I + m * T::TX] = d[m].y;
+          }
+      } else {
+        R d[D];
+        cell_derivs<D, LX, R>(d, sm + T::U + w0, sm + T::U + w0, sm[T::SGNY + q * (CY + 1) + c],
+                              sm[T::SGNY + q * (CY + 1) + c + 1], w);
+#pragma unroll
+        for (int m = 0; m < D; ++m)
+          if (m < mmax) yr[2 * T::I + m * T::TX] = d[m];
+      }
+    }
+    __syncthreads();
+  } else if constexpr (!WALK) {
     // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), item = (row, cell, quantity) ----
     // quantity 0: flux_x = d(E)/dx, Riemann on u; 1: div_x = d(phiG cU)/dx, Riemann
     // on phiG; 2: dvdx, upwinded by sign(cU)

@@ -1,17 +1,17 @@
 // stage_d4_mix.cu -- stage-kernel instantiations for MCV4, split precision:
 // the tile shapes (cells x cells, threads, CTAs per SM the registers must allow,
-// sweep style, TMA-staged persistent form) the autotuner chooses from.
+// TMA-staged persistent form) the autotuner chooses from; split-precision sweeps
+// are per-cell items with packed FP32 pairs.
 #include "mcv_stage.cuh"
 
 namespace mcv {
 
 const StageLauncher *stage_launchers_d4_mix(int *count) {
   static const StageLauncher table[] = {
-    StageConfig<4, 8, 8, 320, 2, true, false>::make(),
-    StageConfig<4, 8, 8, 320, 3, true, false>::make(),
-    StageConfig<4, 8, 8, 256, 4, true, false>::make(),
-    StageConfig<4, 8, 8, 384, 2, true, false>::make(),
-    StageConfig<4, 12, 12, 224, 1, true, true>::make(),
+    StageConfig<4, 8, 8, 320, 2, true, false, false>::make(),
+    StageConfig<4, 8, 8, 320, 3, true, false, false>::make(),
+    StageConfig<4, 8, 8, 256, 3, true, false, false>::make(),
+    StageConfig<4, 8, 8, 384, 2, true, false, false>::make(),
     StageConfig<4, 8, 8, 256, 2, true, false, true>::make(),
     StageConfig<4, 8, 8, 320, 2, true, false, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
