@@ -606,8 +606,8 @@ __global__ void __launch_bounds__(NT, MINB)
 
   if constexpr (TMA) {
     // wait for this item's copies; every thread agrees before anyone leaves
-    const bool ok = mbar_wait_bounded(bar, parity);
-    if (__syncthreads_or(!ok)) {
+    const bool arrived = mbar_wait_bounded(bar, parity);
+    if (__syncthreads_or(!arrived)) {
       if (threadIdx.x == 0) atomicExch(a.err, 1);
       mbar_wait_bounded(bar, parity);  // the copies in flight land before the CTA exits
       return;
@@ -846,12 +846,61 @@ __global__ void __launch_bounds__(NT, MINB)
   const bool last_x = (c0x + ncx == g.Nc), last_y = (c0y + ncy == g.Nc);
   const int qown = last_x ? txe : txe - 1;  // seam points belong to the left / lower tile
   const int rown = last_y ? tye : tye - 1;
-  for (int it = threadIdx.x; it < T::I; it += NT) {
+  // Each thread first loads the global operands of its next CHA points (RK
+  // base, accumulators, input increments, Coriolis), so their latencies
+  // overlap, then assembles and stores them.
+  constexpr int CHA = 2;
+  constexpr bool NEED_BASE = MIXED ? last_stage(KIND) : !first_stage(KIND);
+  constexpr bool NEED_ACC = (KIND == RK4_S2 || KIND == RK4_S3 || KIND == RK4_S4);
+  constexpr bool NEED_INC = MIXED && (KIND == RK3_S2 || KIND == RK3_S3);
+  for (int base0 = 0; base0 < T::I; base0 += NT * CHA) {
+    double gb[CHA][3], ga[CHA][3], gf[CHA];
+    float gd[CHA][3];
+    bool val[CHA];
+#pragma unroll
+    for (int k = 0; k < CHA; ++k) {
+      const int it = base0 + threadIdx.x + k * NT;
+      const int r = it / T::TX, q = it - r * T::TX;
+      val[k] = it < T::I && q < qown && r < rown;
+      if (!val[k]) continue;
+      const long long go = mbase + tbase + ((H + r) * g.P + (H + q));
+      if constexpr (!MIXED) {
+        gf[k] = __ldg(a.fcor + pbase + tbase + ((H + r) * g.P + (H + q)));
+        if constexpr (NEED_BASE) {
+          gb[k][0] = a.u0[go];
+          gb[k][1] = a.v0[go];
+          gb[k][2] = a.p0[go];
+        }
+        if constexpr (NEED_ACC) {
+          ga[k][0] = a.aU[go];
+          ga[k][1] = a.aV[go];
+          ga[k][2] = a.aP[go];
+        }
+      } else {
+        if constexpr (NEED_BASE) {
+          gb[k][0] = a.yu[go];
+          gb[k][1] = a.yv[go];
+          gb[k][2] = a.yp[go];
+        }
+        if constexpr (NEED_ACC) {
+          gd[k][0] = a.fU[go];
+          gd[k][1] = a.fV[go];
+          gd[k][2] = a.fP[go];
+        } else if constexpr (NEED_INC) {
+          gd[k][0] = a.du[go];
+          gd[k][1] = a.dv[go];
+          gd[k][2] = a.dp[go];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < CHA; ++k) {
+    if (!val[k]) continue;
+    const int it = base0 + threadIdx.x + k * NT;
     const int r = it / T::TX, q = it - r * T::TX;
-    if (q >= qown || r >= rown) continue;
     const long long go = mbase + tbase + ((H + r) * g.P + (H + q));
     const R sg = sm[T::SG + it], cu = sm[T::CU + it], cv = sm[T::CV + it];
-    const R fc = MIXED ? sm[T::FC + it] : (R)__ldg(a.fcor + pbase + tbase + ((H + r) * g.P + (H + q)));
+    const R fc = MIXED ? sm[T::FC + it] : (R)gf[k];
     const R rsg = R(1) / sg;
     R flux_x = sm[T::XR + it], dvdx = sm[T::XR + 2 * T::I + it];
     R flux_y = sm[T::YR + it], dudy = sm[T::YR + 2 * T::I + it];
@@ -882,18 +931,18 @@ __global__ void __launch_bounds__(NT, MINB)
           a.aP[go] = tP;
         }
       } else {
-        const double ub = a.u0[go], vb = a.v0[go], pgb = a.p0[go] * sg;
+        const double ub = gb[k][0], vb = gb[k][1], pgb = gb[k][2] * sg;
         if constexpr (KIND == RK4_S2 || KIND == RK4_S3) {
           uo = ub + a.inc * tU;
           vo = vb + a.inc * tV;
           pgo = pgb + a.inc * tP;
-          a.aU[go] = a.aU[go] + 2. * tU;
-          a.aV[go] = a.aV[go] + 2. * tV;
-          a.aP[go] = a.aP[go] + 2. * tP;
+          a.aU[go] = ga[k][0] + 2. * tU;
+          a.aV[go] = ga[k][1] + 2. * tV;
+          a.aP[go] = ga[k][2] + 2. * tP;
         } else if constexpr (KIND == RK4_S4) {
-          uo = ub + a.inc * ((a.aU[go] + tU) * (1. / 6.));
-          vo = vb + a.inc * ((a.aV[go] + tV) * (1. / 6.));
-          pgo = pgb + a.inc * ((a.aP[go] + tP) * (1. / 6.));
+          uo = ub + a.inc * ((ga[k][0] + tU) * (1. / 6.));
+          vo = vb + a.inc * ((ga[k][1] + tV) * (1. / 6.));
+          pgo = pgb + a.inc * ((ga[k][2] + tP) * (1. / 6.));
         } else if constexpr (KIND == RK3_S2) {
           uo = 0.75 * ub + 0.25 * us + a.inc * tU;
           vo = 0.75 * vb + 0.25 * vs + a.inc * tV;
@@ -913,17 +962,17 @@ __global__ void __launch_bounds__(NT, MINB)
       const float tp = tP * rsg;
       float iu, iv, ip;  // increment over Y
       if constexpr (KIND == RK4_S4) {
-        iu = a.wt * ((a.fU[go] + tU) * (1.f / 6.f));
-        iv = a.wt * ((a.fV[go] + tV) * (1.f / 6.f));
-        ip = a.wt * ((a.fP[go] + tp) * (1.f / 6.f));
+        iu = a.wt * ((gd[k][0] + tU) * (1.f / 6.f));
+        iv = a.wt * ((gd[k][1] + tV) * (1.f / 6.f));
+        ip = a.wt * ((gd[k][2] + tp) * (1.f / 6.f));
       } else {
         iu = a.wt * tU;
         iv = a.wt * tV;
         ip = a.wt * tp;
         if constexpr (KIND == RK3_S2 || KIND == RK3_S3) {
-          iu += a.wd * a.du[go];
-          iv += a.wd * a.dv[go];
-          ip += a.wd * a.dp[go];
+          iu += a.wd * gd[k][0];
+          iv += a.wd * gd[k][1];
+          ip += a.wd * gd[k][2];
         }
       }
       if constexpr (KIND == RK4_S1) {
@@ -931,15 +980,15 @@ __global__ void __launch_bounds__(NT, MINB)
         a.fV[go] = tV;
         a.fP[go] = tp;
       } else if constexpr (KIND == RK4_S2 || KIND == RK4_S3) {
-        a.fU[go] = a.fU[go] + 2.f * tU;
-        a.fV[go] = a.fV[go] + 2.f * tV;
-        a.fP[go] = a.fP[go] + 2.f * tp;
+        a.fU[go] = gd[k][0] + 2.f * tU;
+        a.fV[go] = gd[k][1] + 2.f * tV;
+        a.fP[go] = gd[k][2] + 2.f * tp;
       }
       if constexpr (last_stage(KIND)) {
         // FP64 accumulation of the state into the other state buffer
-        uo = a.yu[go] + (double)iu;
-        vo = a.yv[go] + (double)iv;
-        po = a.yp[go] + (double)ip;
+        uo = gb[k][0] + (double)iu;
+        vo = gb[k][1] + (double)iv;
+        po = gb[k][2] + (double)ip;
         a.uo[go] = uo;
         a.vo[go] = vo;
         a.po[go] = po;
@@ -973,6 +1022,7 @@ __global__ void __launch_bounds__(NT, MINB)
         if (gj == nn - 1) b[3 * nn + gi] = val;
       }
     }
+  }
   }
   if constexpr (TMA) __syncthreads();  // the next item reuses the shared arrays
   }
