@@ -76,6 +76,12 @@ int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double *matrixG, 
  * first step reads the caller's halo as src/time_scheme_mod.F90:27 does). */
 int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const double *u, const double *v, const double *phi);
 
+/* Replace member m's state (u, v, phi over the padded range) and keep its
+ * phi_s: the per-step input of a driver that owns the state on the host.
+ * Split precision keeps the member's mean-depth reference (a constant offset
+ * of E that drops out of every derivative). */
+int mcv_set_state(mcv_handle *h, int m, const double *u, const double *v, const double *phi);
+
 /* Advance every member by nsteps RK steps (the loop of src/MCV_SW.F90:57-77
  * without history output).  Blocks until the steps are done. */
 int mcv_step(mcv_handle *h, int nsteps);
@@ -124,7 +130,7 @@ int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, double *halo_m
 /* Stage-kernel tile shapes the autotuner timed on this handle's grid (it runs
  * once, before the first step): ncand (at most 16) candidates,
  * shapes[5*i..] = {cells in x, cells in y, threads, sweep style (0 per-cell
- * items, 1 line walks), CTAs per SM the kernel's registers allow}, ms[i] =
+ * items, n walks of n cells), CTAs per SM the kernel's registers allow}, ms[i] =
  * device time per launch, *chosen = the index in use.  No counterpart in the
  * reference (which has no GPU path). */
 int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, float *ms);

@@ -53,6 +53,7 @@ def lib():
                                       ctypes.c_double, ctypes.c_int, ctypes.POINTER(vp)]),
         "mcv_set_geometry": (ctypes.c_int, [vp, _D, _D, _D, _D, _D, _D, _I, _D]),
         "mcv_set_member": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
+        "mcv_set_state": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D]),
         "mcv_step": (ctypes.c_int, [vp, ctypes.c_int]),
         "mcv_step_async": (ctypes.c_int, [vp, ctypes.c_int]),
         "mcv_sync": (ctypes.c_int, [vp]),
@@ -267,6 +268,10 @@ class Stepper:
     def set_member(self, m, phi_s, u, v, phi):
         arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (phi_s, u, v, phi)]
         _check(lib().mcv_set_member(self.h, int(m), *[_dp(x) for x in arrs]))
+
+    def set_state(self, m, u, v, phi):
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v, phi)]
+        _check(lib().mcv_set_state(self.h, int(m), *[_dp(x) for x in arrs]))
 
     def step(self, nsteps=1):
         _check(lib().mcv_step(self.h, int(nsteps)))

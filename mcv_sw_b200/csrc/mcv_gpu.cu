@@ -814,6 +814,23 @@ extern "C" int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const d
   return MCV_OK;
 }
 
+extern "C" int mcv_set_state(mcv_handle *h, int m, const double *u, const double *v, const double *phi) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (m < 0 || m >= h->members) return fail(MCV_ERR_ARG, "member index out of range");
+  if (!u || !v || !phi) return fail(MCV_ERR_ARG, "state array is NULL");
+  if (!h->member_set[m]) return fail(MCV_ERR_ORDER, "mcv_set_member must precede mcv_set_state");
+  const long long off = (long long)m * h->g.mstride;
+  if (h->mixed) h->mcur[m] = h->cur;
+  double *const *Y = state(h, m);
+  int rc;
+  if ((rc = upload_padded(h, Y[0] + off, u, 8))) return rc;
+  if ((rc = upload_padded(h, Y[1] + off, v, 8))) return rc;
+  if ((rc = upload_padded(h, Y[2] + off, phi, 8))) return rc;
+  MCV_CUDA(cudaStreamSynchronize(h->stream), "state upload");
+  h->steps_done[m] = 0;
+  return MCV_OK;
+}
+
 extern "C" int mcv_step_async(mcv_handle *h, int nsteps) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   if (nsteps < 0) return fail(MCV_ERR_ARG, "nsteps must be >= 0");
@@ -940,11 +957,13 @@ extern "C" int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double 
     for (double *fld : fields) {
       if (!fld) continue;
       for (int p = 0; p < 6; ++p)
-        for (int j = 0; j < npx; ++j)
-          for (int i = 0; i < npx; ++i) {
-            const bool xh = i < H || i >= npx - H, yh = j < H || j >= npx - H;
-            if (xh && yh) fld[(size_t)i + (size_t)npx * ((size_t)j + (size_t)npx * p)] = -9999999999999999.;
-          }
+        for (int cj = 0; cj < 2; ++cj)  // the four H x H corner squares of each panel
+          for (int ci = 0; ci < 2; ++ci)
+            for (int j = 0; j < H; ++j)
+              for (int i = 0; i < H; ++i) {
+                const size_t ii = ci ? (size_t)(npx - H + i) : (size_t)i, jj = cj ? (size_t)(npx - H + j) : (size_t)j;
+                fld[ii + (size_t)npx * (jj + (size_t)npx * p)] = -9999999999999999.;
+              }
     }
   }
   if (phiG)
@@ -1059,7 +1078,7 @@ extern "C" int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, f
       shapes[5 * i] = h->cands[i].CX;
       shapes[5 * i + 1] = h->cands[i].CY;
       shapes[5 * i + 2] = h->cands[i].NT;
-      shapes[5 * i + 3] = h->cands[i].walk ? 1 : 0;
+      shapes[5 * i + 3] = h->cands[i].walk;
       shapes[5 * i + 4] = h->cands[i].minb;
     }
     if (ms) ms[i] = h->tune_ms[i];

@@ -224,8 +224,11 @@ __device__ __forceinline__ void cell_derivs2(float2 out[D], const float2 *f, con
 // Walking the line carries the previous cell's one-sided derivatives, so each
 // interface flux is formed once; it is the value both neighbouring cells'
 // calc_tendP calls produce.  SAME: f and q are the same field (dvdx, dudy).
+// The walk's last point is written only when the walk ends the line (`ends`):
+// otherwise it is the next walk's first point, which that walk writes (one
+// writer per point).
 template <int D, int NMAX, int S, int OS, bool SAME, typename R>
-__device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, int ncells, R *out,
+__device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, int ncells, bool ends, R *out,
                                           const Widths<R> &w) {
   const R ip = (D == 3) ? w.inv_dx : w.inv_2dx;
   R cf[D], cq[D];
@@ -283,7 +286,7 @@ __device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, 
       }
 #pragma unroll
       for (int m = 0; m < D - 1; ++m) out[(c * (D - 1) + m) * OS] = o[m];
-      if (c == ncells - 1) out[(c * (D - 1) + D - 1) * OS] = o[D - 1];
+      if (c == ncells - 1 && ends) out[(c * (D - 1) + D - 1) * OS] = o[D - 1];
 #pragma unroll
       for (int m = 0; m < D; ++m) {
         cf[m] = nf[m];
@@ -291,6 +294,80 @@ __device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, 
       }
       fR = polyfit_right<D>(cf, ip);
       qR = SAME ? fR : polyfit_right<D>(cq, ip);
+      fluxL = fluxR;
+    }
+  }
+}
+
+// The interior points of one cell from its end derivatives (packed pairs):
+// the MCV constraint of calc_tendP (src/spatial_operators_mod.F90:179-200).
+template <int D, int S>
+__device__ __forceinline__ void cell_interior2(float2 o[D], const float2 *c, const Widths<float> &w) {
+  const float2 via = mul2(fma2(bc2(-1.f), c[0], c[(D - 1) * S]), bc2(w.inv_dx));
+  if constexpr (D == 3) {
+    o[1] = fma2(bc2(1.5f), via, mul2(bc2(-0.25f), add2(o[0], o[2])));
+  } else {
+    const float2 t = fma2(bc2(-1.f), c[2 * S], fma2(bc2(-1.f), c[S], add2(c[0], c[3 * S])));
+    const float2 k = mul2(bc2(2.f / 3.f), mul2(t, bc2(w.inv_dx)));
+    float2 a = fma2(bc2(-4.f / 27.f), o[0], mul2(bc2(4.f / 3.f), via));
+    o[1] = fma2(bc2(-1.f), k, fma2(bc2(-5.f / 27.f), o[3], a));
+    a = fma2(bc2(-5.f / 27.f), o[0], mul2(bc2(4.f / 3.f), via));
+    o[2] = add2(k, fma2(bc2(-4.f / 27.f), o[3], a));
+  }
+}
+
+// line_walk for two quantities at once (packed FP32 pairs, one eigenvalue per
+// interface): f and q point to the first point of the halo cell before the
+// walk, results go to outx (first of the pair) and outy (second).
+template <int D, int NMAX, int S, int OS>
+__device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, const float *lam, int ncells, bool ends,
+                                           float *outx, float *outy, const Widths<float> &w) {
+  const float2 ip = bc2((D == 3) ? w.inv_dx : w.inv_2dx);
+  float2 cf[D], cq[D];
+#pragma unroll
+  for (int m = 0; m < D; ++m) {
+    cf[m] = f[m * S];
+    cq[m] = q[m * S];
+  }
+  float2 fR = polyfit_right2<D>(cf, ip), qR = polyfit_right2<D>(cq, ip);
+#pragma unroll
+  for (int m = 0; m < D; ++m) {
+    cf[m] = f[(D - 1 + m) * S];
+    cq[m] = q[(D - 1 + m) * S];
+  }
+  float2 fluxL = riemann2(fR, polyfit_left2<D>(cf, ip), qR, polyfit_left2<D>(cq, ip), lam[0]);
+  fR = polyfit_right2<D>(cf, ip);
+  qR = polyfit_right2<D>(cq, ip);
+#pragma unroll
+  for (int c = 0; c < NMAX; ++c) {
+    if (c < ncells) {
+      float2 nf[D], nq[D];
+#pragma unroll
+      for (int m = 0; m < D; ++m) {
+        nf[m] = f[((c + 2) * (D - 1) + m) * S];
+        nq[m] = q[((c + 2) * (D - 1) + m) * S];
+      }
+      const float2 fluxR = riemann2(fR, polyfit_left2<D>(nf, ip), qR, polyfit_left2<D>(nq, ip), lam[c + 1]);
+      float2 o[D];
+      o[0] = fluxL;
+      o[D - 1] = fluxR;
+      cell_interior2<D, 1>(o, cf, w);
+#pragma unroll
+      for (int m = 0; m < D - 1; ++m) {
+        outx[(c * (D - 1) + m) * OS] = o[m].x;
+        outy[(c * (D - 1) + m) * OS] = o[m].y;
+      }
+      if (c == ncells - 1 && ends) {
+        outx[(c * (D - 1) + D - 1) * OS] = o[D - 1].x;
+        outy[(c * (D - 1) + D - 1) * OS] = o[D - 1].y;
+      }
+#pragma unroll
+      for (int m = 0; m < D; ++m) {
+        cf[m] = nf[m];
+        cq[m] = nq[m];
+      }
+      fR = polyfit_right2<D>(cf, ip);
+      qR = polyfit_right2<D>(cq, ip);
       fluxL = fluxR;
     }
   }
@@ -382,12 +459,13 @@ __device__ __forceinline__ void mix_point(MixPoint &o, const double4 mx, const d
 }
 
 // MINB: CTAs per SM the register allocation must allow (launch bounds).
+// WALK: 0 -- sweeps as per-cell items; n -- sweeps as walks of n cells.
 // TMA: persistent form -- each CTA walks work items (tile, panel, member)
 // blockIdx.x, blockIdx.x + gridDim.x, ...; the next item's input fields are
 // copied into a shared-memory staging area by TMA while the current item's
 // sweeps and update run.  Otherwise one CTA per (tile, panel, member) loads
 // its fields with ordinary loads.
-template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, bool WALK, bool TMA>
+template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA>
 __global__ void __launch_bounds__(NT, MINB)
     stage_kernel(const GridDesc g, const StageArgs a, const __grid_constant__ TileMaps tm) {
   using R = std::conditional_t<MIXED, float, double>;
@@ -707,8 +785,47 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   const Widths<R> w(g);
 
-  if constexpr (MIXED) {
-    static_assert(!WALK, "split precision sweeps are per-cell items");
+  if constexpr (MIXED && WALK > 0) {
+    // ---- phase W (split precision): walks of WALK cells, item = (line,
+    // segment, kind); kind 0: the (E, phiG c^i) pair with Riemann on (wind
+    // component, phiG); kind 1: dvdx / dudy upwinded by sign(c^i)
+    constexpr int SEGX = WALK < CX ? WALK : CX, SEGY = WALK < CY ? WALK : CY;
+    constexpr int NSX = (CX + SEGX - 1) / SEGX, NSY = (CY + SEGY - 1) / SEGY;
+    const float2 *s2 = reinterpret_cast<const float2 *>(sm);
+    for (int it = threadIdx.x; it < 2 * (T::TY * NSX + T::TX * NSY); it += NT) {
+      if (it < 2 * T::TY * NSX) {
+        const int r = it % T::TY, rest = it / T::TY;
+        const int sx = rest % NSX, kk = rest / NSX;
+        const int c0 = sx * SEGX;
+        if (r >= tye || c0 >= ncx) continue;
+        const int nseg = min(SEGX, ncx - c0), w0 = (r + H) * LX + c0 * (D - 1);
+        const bool ends = c0 + nseg == ncx;
+        R *xr = sm + T::XR + r * T::TX + c0 * (D - 1);
+        if (kk == 0)
+          line_walk2<D, SEGX, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, sm + T::LAMX + r * (CX + 1) + c0, nseg,
+                                    ends, xr, xr + T::I, w);
+        else
+          line_walk<D, SEGX, 1, 1, true, R>(sm + T::V + w0, sm + T::V + w0, sm + T::SGNX + r * (CX + 1) + c0, nseg,
+                                            ends, xr + 2 * T::I, w);
+      } else {
+        const int j = it - 2 * T::TY * NSX;
+        const int q = j % T::TX, rest = j / T::TX;
+        const int sy = rest % NSY, kk = rest / NSY;
+        const int c0 = sy * SEGY;
+        if (q >= txe || c0 >= ncy) continue;
+        const int nseg = min(SEGY, ncy - c0), w0 = c0 * (D - 1) * LX + (q + H);
+        const bool ends = c0 + nseg == ncy;
+        R *yr = sm + T::YR + q + c0 * (D - 1) * T::TX;
+        if (kk == 0)
+          line_walk2<D, SEGY, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, sm + T::LAMY + q * (CY + 1) + c0,
+                                         nseg, ends, yr, yr + T::I, w);
+        else
+          line_walk<D, SEGY, LX, T::TX, true, R>(sm + T::U + w0, sm + T::U + w0, sm + T::SGNY + q * (CY + 1) + c0,
+                                                 nseg, ends, yr + 2 * T::I, w);
+      }
+    }
+    __syncthreads();
+  } else if constexpr (MIXED) {
     // ---- phase X: x-sweep (spatial_operators_mod.F90:63-93), item = (row, cell, kind) ----
     // kind 0: flux_x = d(E)/dx (Riemann on u) and div_x = d(phiG cU)/dx (Riemann
     // on phiG) as one float2 pair; kind 1: dvdx, upwinded by sign(cU)
@@ -810,33 +927,49 @@ __global__ void __launch_bounds__(NT, MINB)
     __syncthreads();
   } else {
     // ---- phase W: x-walks along rows (spatial_operators_mod.F90:63-93) and
-    // y-walks down columns (:95-125), one item per (line, quantity):
-    // quantity 0: flux = d(E)/dx^i, Riemann on the covariant wind component;
-    // 1: div = d(phiG c^i)/dx^i, Riemann on phiG; 2: dvdx / dudy upwinded by sign(c^i)
-    for (int it = threadIdx.x; it < 3 * (T::TY + T::TX); it += NT) {
-      if (it < 3 * T::TY) {
-        const int r = it % T::TY, k = it / T::TY;
-        if (r >= tye) continue;
-        const R *row = sm + (r + H) * LX;
-        R *xr = sm + T::XR + k * T::I + r * T::TX;
+    // y-walks down columns (:95-125), one item per (line, segment of WALK
+    // cells, quantity): quantity 0: flux = d(E)/dx^i, Riemann on the covariant
+    // wind component; 1: div = d(phiG c^i)/dx^i, Riemann on phiG; 2: dvdx /
+    // dudy upwinded by sign(c^i).  A walk forms each interface flux inside its
+    // segment once.
+    constexpr int SEGX = WALK < CX ? WALK : CX, SEGY = WALK < CY ? WALK : CY;
+    constexpr int NSX = (CX + SEGX - 1) / SEGX, NSY = (CY + SEGY - 1) / SEGY;
+    for (int it = threadIdx.x; it < 3 * (T::TY * NSX + T::TX * NSY); it += NT) {
+      if (it < 3 * T::TY * NSX) {
+        const int r = it % T::TY, rest = it / T::TY;
+        const int sx = rest % NSX, k = rest / NSX;
+        const int c0 = sx * SEGX;
+        if (r >= tye || c0 >= ncx) continue;
+        const int nseg = min(SEGX, ncx - c0);
+        const R *row = sm + (r + H) * LX + c0 * (D - 1);
+        R *xr = sm + T::XR + k * T::I + r * T::TX + c0 * (D - 1);
+        const R *lam = sm + T::LAMX + r * (CX + 1) + c0;
+        const bool ends = c0 + nseg == ncx;
         if (k == 0)
-          line_walk<D, CX, 1, 1, false, R>(row + T::E, row + T::U, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
+          line_walk<D, SEGX, 1, 1, false, R>(row + T::E, row + T::U, lam, nseg, ends, xr, w);
         else if (k == 1)
-          line_walk<D, CX, 1, 1, false, R>(row + T::PGU, row + T::PG, sm + T::LAMX + r * (CX + 1), ncx, xr, w);
+          line_walk<D, SEGX, 1, 1, false, R>(row + T::PGU, row + T::PG, lam, nseg, ends, xr, w);
         else
-          line_walk<D, CX, 1, 1, true, R>(row + T::V, row + T::V, sm + T::SGNX + r * (CX + 1), ncx, xr, w);
+          line_walk<D, SEGX, 1, 1, true, R>(row + T::V, row + T::V, sm + T::SGNX + r * (CX + 1) + c0, nseg, ends,
+                                            xr, w);
       } else {
-        const int j = it - 3 * T::TY;
-        const int q = j % T::TX, k = j / T::TX;
-        if (q >= txe) continue;
-        const R *col = sm + (q + H);
-        R *yr = sm + T::YR + k * T::I + q;
+        const int j = it - 3 * T::TY * NSX;
+        const int q = j % T::TX, rest = j / T::TX;
+        const int sy = rest % NSY, k = rest / NSY;
+        const int c0 = sy * SEGY;
+        if (q >= txe || c0 >= ncy) continue;
+        const int nseg = min(SEGY, ncy - c0);
+        const R *col = sm + (q + H) + c0 * (D - 1) * LX;
+        R *yr = sm + T::YR + k * T::I + q + c0 * (D - 1) * T::TX;
+        const R *lam = sm + T::LAMY + q * (CY + 1) + c0;
+        const bool ends = c0 + nseg == ncy;
         if (k == 0)
-          line_walk<D, CY, LX, T::TX, false, R>(col + T::E, col + T::V, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
+          line_walk<D, SEGY, LX, T::TX, false, R>(col + T::E, col + T::V, lam, nseg, ends, yr, w);
         else if (k == 1)
-          line_walk<D, CY, LX, T::TX, false, R>(col + T::PGV, col + T::PG, sm + T::LAMY + q * (CY + 1), ncy, yr, w);
+          line_walk<D, SEGY, LX, T::TX, false, R>(col + T::PGV, col + T::PG, lam, nseg, ends, yr, w);
         else
-          line_walk<D, CY, LX, T::TX, true, R>(col + T::U, col + T::U, sm + T::SGNY + q * (CY + 1), ncy, yr, w);
+          line_walk<D, SEGY, LX, T::TX, true, R>(col + T::U, col + T::U, sm + T::SGNY + q * (CY + 1) + c0, nseg,
+                                                 ends, yr, w);
       }
     }
     __syncthreads();
@@ -1036,7 +1169,7 @@ using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const GridDesc &g, con
 
 struct StageLauncher {
   int CX, CY, NT, minb;
-  bool walk;  // sweeps as line walks instead of per-cell items
+  int walk;   // 0: sweeps as per-cell items; n: walks of n cells
   bool tma;   // persistent CTAs with TMA-staged tiles
   size_t smem;
   int box_x, box_y;         // staged box of one field (TMA form)
@@ -1045,7 +1178,7 @@ struct StageLauncher {
   int (*blocks_per_sm)();   // resident CTAs per SM (sizes the persistent grid)
 };
 
-template <int D, int CX, int CY, int NT, int MINB, bool MIXED, bool WALK, bool TMA = false>
+template <int D, int CX, int CY, int NT, int MINB, bool MIXED, int WALK, bool TMA = false>
 struct StageConfig {
   using T = Tile<D, CX, CY, std::conditional_t<MIXED, float, double>>;
   static constexpr size_t SMEM = TMA ? T::bytes_tma(MIXED) : T::bytes(MIXED);

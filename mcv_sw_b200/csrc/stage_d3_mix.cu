@@ -1,18 +1,21 @@
 // stage_d3_mix.cu -- stage-kernel instantiations for MCV3, split precision:
 // the tile shapes (cells x cells, threads, CTAs per SM the registers must allow,
-// TMA-staged persistent form) the autotuner chooses from; split-precision sweeps
-// are per-cell items with packed FP32 pairs.
+// sweep style (0: per-cell items, n: walks of n cells), TMA-staged persistent
+// form) the autotuner chooses from; split-precision sweeps run on packed FP32
+// pairs.
 #include "mcv_stage.cuh"
 
 namespace mcv {
 
 const StageLauncher *stage_launchers_d3_mix(int *count) {
   static const StageLauncher table[] = {
-    StageConfig<3, 12, 12, 320, 2, true, false, false>::make(),
-    StageConfig<3, 12, 12, 320, 3, true, false, false>::make(),
-    StageConfig<3, 12, 12, 256, 3, true, false, false>::make(),
-    StageConfig<3, 16, 12, 448, 2, true, false, false>::make(),
-    StageConfig<3, 12, 12, 320, 2, true, false, true>::make()};
+    StageConfig<3, 12, 12, 320, 2, true, 0>::make(),
+    StageConfig<3, 12, 12, 320, 3, true, 0>::make(),
+    StageConfig<3, 12, 12, 256, 3, true, 0>::make(),
+    StageConfig<3, 12, 12, 320, 2, true, 2>::make(),
+    StageConfig<3, 16, 12, 448, 2, true, 0>::make(),
+    StageConfig<3, 12, 12, 320, 2, true, 0, true>::make(),
+    StageConfig<3, 12, 12, 320, 2, true, 2, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }

@@ -1,19 +1,21 @@
 // stage_d4_mix.cu -- stage-kernel instantiations for MCV4, split precision:
 // the tile shapes (cells x cells, threads, CTAs per SM the registers must allow,
-// TMA-staged persistent form) the autotuner chooses from; split-precision sweeps
-// are per-cell items with packed FP32 pairs.
+// sweep style (0: per-cell items, n: walks of n cells), TMA-staged persistent
+// form) the autotuner chooses from; split-precision sweeps run on packed FP32
+// pairs.
 #include "mcv_stage.cuh"
 
 namespace mcv {
 
 const StageLauncher *stage_launchers_d4_mix(int *count) {
   static const StageLauncher table[] = {
-    StageConfig<4, 8, 8, 320, 2, true, false, false>::make(),
-    StageConfig<4, 8, 8, 320, 3, true, false, false>::make(),
-    StageConfig<4, 8, 8, 256, 3, true, false, false>::make(),
-    StageConfig<4, 8, 8, 384, 2, true, false, false>::make(),
-    StageConfig<4, 8, 8, 256, 2, true, false, true>::make(),
-    StageConfig<4, 8, 8, 320, 2, true, false, true>::make()};
+    StageConfig<4, 8, 8, 320, 2, true, 0>::make(),
+    StageConfig<4, 8, 8, 320, 3, true, 0>::make(),
+    StageConfig<4, 8, 8, 256, 3, true, 0>::make(),
+    StageConfig<4, 8, 8, 320, 2, true, 2>::make(),
+    StageConfig<4, 8, 8, 256, 2, true, 0, true>::make(),
+    StageConfig<4, 8, 8, 320, 2, true, 0, true>::make(),
+    StageConfig<4, 8, 8, 320, 2, true, 2, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }

@@ -136,3 +136,30 @@ def test_every_tile_shape_agrees(order):
             a, b = interior(outs[i][k], H, n), interior(outs[0][k], H, n)
             d = np.abs(a - b).max() / np.abs(b).max()
             assert d < TILE_TOL, (i, k, d)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_set_state_replaces_the_state(precision):
+    """mcv_set_state (u, v, phi only) continues like mcv_set_member with the
+    same phi_s: bit for bit in FP64; split precision keeps the first state's
+    mean-depth reference, a constant offset of E that drops out of the
+    derivatives (rounding-level difference)."""
+    geom = api.Geometry(4, 8, cases.EARTH_RADIUS)
+    a, _ = cases.small(seed=3, nc=8, order=4, geom=geom)
+    b, _ = cases.small(seed=4, nc=8, order=4, geom=geom)
+    outs = []
+    for first in (a, b):
+        with api.Stepper(4, 8, a.dt, "RK4", precision=precision, radius=cases.EARTH_RADIUS) as s:
+            s.set_geometry(geom)
+            s.select_tile(0)
+            s.set_member(0, b.phi_s, first.u, first.v, first.phi)
+            if first is a:
+                s.set_state(0, b.u, b.v, b.phi)
+            s.step(3)
+            outs.append(s.get_state(0))
+    H, n = geom.H, geom.n
+    for k in ("u", "v", "phi"):
+        if precision == "fp64":
+            assert np.array_equal(outs[0][k], outs[1][k]), k
+        else:
+            assert rel_l2(interior(outs[0][k], H, n), interior(outs[1][k], H, n)) < 1e-12, k
