@@ -60,6 +60,22 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest x over the ranks: the job's time is its slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, steps, dt, ms):
+    """Whole-job simulated days per second: each of `world` ranks advances its
+    own replica by `steps` steps of dt seconds within the job's ms."""
+    return world * steps * dt / 86400.0 / (ms / 1e3)
+
+
 def build_workload(name):
     from mcv_sw_b200 import cases
     if name == "large":
@@ -225,11 +241,8 @@ def time_path(args, st, geom, precision, world, barrier, dist, local):
     ms = s.time_steps(args.steps)
     barrier()
     clk = clocks.stop()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps * st.dt / 86400.0 / (ms / 1e3)
+    ms = max_over_ranks(ms, dist)
+    value = replica_value(world, args.steps, st.dt, ms)
     stage_ms, halo_ms = s.profile_step(3)
     per_pv = stage_bytes(st.scheme, precision)
     achieved = sum(b * n_pv for b in per_pv) / (sum(stage_ms) * 1e-3) / 1e9
@@ -376,10 +389,7 @@ def run_ours(args):
         main.get_state(0, out=ho)
     barrier()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
     field_bytes = 8 * 6 * geom.npx * geom.npx
     e2e = {"value": world * args.e2e_steps * st.dt / 86400.0 / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": 3 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
