@@ -405,12 +405,12 @@ int launch_stage(mcv_handle *h, int cand, int s, int c) {
   const int kind = stage_kind(h, s);
   TileMaps tm;
   std::memset(&tm, 0, sizeof(tm));
+  tm.total = g.tiles_x * g.tiles_y * 6 * h->n_active;  // work items (tile, panel, member)
   if (!L.tma) {
     L.launch[kind](dim3(g.tiles_x * g.tiles_y, 6, h->n_active), h->stream, g, a, tm);
     return MCV_OK;
   }
   if (int rc = stage_maps(h, L, a, kind, tm)) return rc;
-  tm.total = g.tiles_x * g.tiles_y * 6 * h->n_active;
   const int ctas = std::max(1, std::min(tm.total, h->bps[cand] * h->nsm));
   L.launch[kind](dim3(ctas), h->stream, g, a, tm);
   return MCV_OK;

@@ -82,6 +82,9 @@ template <int D, bool MIXED>
 __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloArgs a) {
   constexpr int H = D - 1;
   const int n = g.n;
+  // the next stage kernel may launch now: its items clear of the panel edges
+  // read nothing this kernel writes, the others wait for its completion
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   // one thread per (member, panel, edge, halo line h = 0..H, position k)
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long per_member = 24LL * (H + 1) * n;

@@ -458,6 +458,50 @@ __device__ __forceinline__ void mix_point(MixPoint &o, const double4 mx, const d
   o.fc = two_omega * (panel < 4 ? my.x * rinv : (panel == 4 ? rinv : -rinv));
 }
 
+// Work item wi of a TMA-form launch -> tile (tx, ty), panel and active-member
+// slot.  Items whose tiles lie away from the panel edges come first: with
+// programmatic dependent launch they start while the previous halo kernel
+// still runs (they read nothing it writes), and the edge items, which wait for
+// it, come last.  nslots = active members of the launch.
+struct WorkItem {
+  int tx, ty, panel, slot;
+};
+__device__ __forceinline__ WorkItem decode_item(int wi, int tiles_x, int tiles_y, int nslots) {
+  const int ix = max(tiles_x - 2, 0), iy = max(tiles_y - 2, 0);
+  const int nin = ix * iy, nedge = tiles_x * tiles_y - nin;
+  WorkItem w;
+  int ps;
+  if (wi < nin * 6 * nslots) {
+    ps = wi / nin;
+    const int r = wi - ps * nin;
+    w.tx = 1 + r % ix;
+    w.ty = 1 + r / ix;
+  } else {
+    const int wj = wi - nin * 6 * nslots;
+    ps = wj / nedge;
+    const int e = wj - ps * nedge;
+    if (e < tiles_x) {
+      w.tx = e;
+      w.ty = 0;
+    } else if (e < 2 * tiles_x) {
+      w.tx = e - tiles_x;
+      w.ty = tiles_y - 1;
+    } else {
+      const int f = e - 2 * tiles_x;
+      w.tx = (f < iy) ? 0 : tiles_x - 1;
+      w.ty = 1 + ((f < iy) ? f : f - iy);
+    }
+  }
+  w.panel = ps % 6;
+  w.slot = ps / 6;
+  return w;
+}
+
+// PTX programmatic dependent launch: wait until the preceding kernel (the halo
+// kernel) has completed and its writes are visible; let the next kernel launch.
+__device__ __forceinline__ void wait_prerequisite_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // MINB: CTAs per SM the register allocation must allow (launch bounds).
 // WALK: 0 -- sweeps as per-cell items; n -- sweeps as walks of n cells.
 // TMA: persistent form -- each CTA walks work items (tile, panel, member)
@@ -484,10 +528,24 @@ __global__ void __launch_bounds__(NT, MINB)
   constexpr int NF = MIXED ? (first_stage(KIND) ? 4 : 7) : 8;
 
   // TMA: issue the copies of work item wi's input fields (one thread)
+  const int nslots = tm.total / (ntile * 6);
+  // the loaded rectangle of tile (tx, ty) reaches a panel boundary line or the
+  // halo, which the previous halo kernel writes
+  auto touches_edge = [&](int tx, int ty) {
+    const int cx = min(CX, g.Nc - tx * CX), cy = min(CY, g.Nc - ty * CY);
+    const int x0 = tx * CX * (D - 1) - H, x1 = tx * CX * (D - 1) + cx * (D - 1) + H;  // interior indices
+    const int y0 = ty * CY * (D - 1) - H, y1 = ty * CY * (D - 1) + cy * (D - 1) + H;
+    return x0 < 1 || y0 < 1 || x1 > g.n - 2 || y1 > g.n - 2;
+  };
+  bool waited = false;  // TMA form, thread 0: the prerequisite grid has completed
   auto issue = [&](int wi) {
-    const int tile = wi % ntile, rest = wi / ntile;
-    const int panel = rest % 6, mem = __ldg(a.active + rest / 6);
-    const int X0 = (tile % g.tiles_x) * CX * (D - 1), Y0 = (tile / g.tiles_x) * CY * (D - 1);
+    const WorkItem it = decode_item(wi, g.tiles_x, g.tiles_y, nslots);
+    if (!waited && touches_edge(it.tx, it.ty)) {
+      wait_prerequisite_grid();
+      waited = true;
+    }
+    const int panel = it.panel, mem = __ldg(a.active + it.slot);
+    const int X0 = it.tx * CX * (D - 1), Y0 = it.ty * CY * (D - 1);
     uint32_t bytes = 0;
 #pragma unroll
     for (int f = 0; f < NF; ++f) bytes += T::field_bytes(MIXED, f);
@@ -519,18 +577,22 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   const int wfirst = TMA ? (int)blockIdx.x : 0, wstep = TMA ? (int)gridDim.x : 1, wend = TMA ? tm.total : 1;
   for (int wi = wfirst; wi < wend; wi += wstep) {
-  int tile, panel, mem;
+  int tx, ty, panel, mem;
   if constexpr (TMA) {
-    tile = wi % ntile;
-    const int rest = wi / ntile;
-    panel = rest % 6;
-    mem = __ldg(a.active + rest / 6);
+    const WorkItem item = decode_item(wi, g.tiles_x, g.tiles_y, nslots);
+    tx = item.tx;
+    ty = item.ty;
+    panel = item.panel;
+    mem = __ldg(a.active + item.slot);
   } else {
-    tile = blockIdx.x;
+    // one CTA per (tile, panel, member) in panel order, which keeps the
+    // neighbours' halo reads in L2; it starts once the previous kernel is done
+    tx = blockIdx.x % g.tiles_x;
+    ty = blockIdx.x / g.tiles_x;
     panel = blockIdx.y;
     mem = __ldg(a.active + blockIdx.z);
+    wait_prerequisite_grid();
   }
-  const int tx = tile % g.tiles_x, ty = tile / g.tiles_x;
   const int c0x = tx * CX, c0y = ty * CY;
   const int ncx = min(CX, g.Nc - c0x), ncy = min(CY, g.Nc - c0y);
   const int X0 = c0x * (D - 1), Y0 = c0y * (D - 1);  // padded coords of the first loaded point
@@ -1185,9 +1247,22 @@ struct StageConfig {
   // TMA box x coordinates are tile origins X0 = tile * CX * (D - 1): their byte
   // offsets must be multiples of 16 (FP32 fields: X0 % 4 == 0; FP64: even)
   static_assert(!TMA || (CX * (D - 1)) % (MIXED ? 4 : 2) == 0, "TMA box origin not 16-byte aligned");
+  // launched with programmatic stream serialization: the kernel's CTAs may
+  // become resident while the preceding halo kernel finishes (TMA form: items
+  // clear of the panel edges also run then; the rest wait for it)
   template <int KIND>
   static void launch(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a, const TileMaps &tm) {
-    stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA><<<grid, NT, SMEM, s>>>(g, a, tm);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA>, g, a, tm);
   }
   template <int KIND>
   static cudaError_t attr() {
