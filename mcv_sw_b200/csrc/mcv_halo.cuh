@@ -115,32 +115,72 @@ __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloA
     }
   };
 
+  // destination point and its rotation, loaded ahead of the dependent loads
+  int di, dj;
+  strip_point(e, -h, k, n, di, dj);
+  const long long o = mb + p * g.plane + (long long)(dj + H) * g.P + (di + H);
+  const double4 N = a.Ntab[((p * 4 + e) * (H + 1) + h) * n + k];
+  double yu_d = 0., yv_d = 0., yp_d = 0.;
+  if constexpr (MIXED) {
+    yu_d = a.u[o];
+    yv_d = a.v[o];
+    yp_d = a.phi[o];
+  }
+
   double zw, mw, ph;
   if (h > 0) {
     // halo line h: neighbour line h rotated to the sphere, interpolated along
-    // the edge, rotated back to this panel (ghost_mod.f90:154-181)
+    // the edge, rotated back to this panel (ghost_mod.f90:154-181).  The D
+    // neighbour points' loads are all issued before any is used: a point at an
+    // end of the line is a boundary point and takes its raw copy; the state
+    // load of such a point goes to its inner neighbour instead (FP64 form: the
+    // boundary itself is rewritten by this kernel) and is not used.
     const int iref = a.giref[(h - 1) * n + k];
     const double2 cc = a.gcoef[(h - 1) * n + k];
-    double qz[D], qm[D], qp[D];
+    double yu[D], yv[D], yp[D];
+    double4 M[D], bv[D];
+    float4 b32[D];
+    float du[D], dv[D], dp[D];
+    bool isb[D];
 #pragma unroll
     for (int m = 0; m < D; ++m) {
       const int kk = (iref - 1) * (D - 1) + m;
       const int ks = L.rev ? n - 1 - kk : kk;
+      isb[m] = (ks == 0 || ks == n - 1);
       int si, sj;
       strip_point(e2, h, ks, n, si, sj);
-      double su, sv, sp;
-      if (ks == 0 || ks == n - 1) {
-        raw_boundary(q, si, sj, su, sv, sp);
+      const int bslot = boundary_slot(si, sj, n);
+      const int kc = MIXED ? ks : min(max(ks, 1), n - 2);
+      strip_point(e2, h, kc, n, si, sj);
+      const long long os = mb + q * g.plane + (long long)(sj + H) * g.P + (si + H);
+      yu[m] = a.u[os];
+      yv[m] = a.v[os];
+      yp[m] = a.phi[os];
+      if constexpr (MIXED) {
+        b32[m] = a.bnd32[bb + q * 4 * n + bslot];
+        du[m] = a.du[os];
+        dv[m] = a.dv[os];
+        dp[m] = a.dp[os];
       } else {
-        const long long o = mb + q * g.plane + (long long)(sj + H) * g.P + (si + H);
-        su = a.u[o]; sv = a.v[o]; sp = a.phi[o];
-        if constexpr (MIXED) {
-          su += (double)a.du[o]; sv += (double)a.dv[o]; sp += (double)a.dp[o];
-        }
+        bv[m] = a.bnd[bb + q * 4 * n + bslot];
       }
-      const double4 M = a.Mtab[((q * 4 + e2) * (H + 1) + h) * n + ks];
-      qz[m] = M.x * su + M.z * sv;  // covProjPlane2Sphere, projection_mod.F90:79-96
-      qm[m] = M.y * su + M.w * sv;
+      M[m] = a.Mtab[((q * 4 + e2) * (H + 1) + h) * n + ks];
+    }
+    double qz[D], qm[D], qp[D];
+#pragma unroll
+    for (int m = 0; m < D; ++m) {
+      double su, sv, sp;
+      if constexpr (MIXED) {
+        su = yu[m] + (double)(isb[m] ? b32[m].x : du[m]);
+        sv = yv[m] + (double)(isb[m] ? b32[m].y : dv[m]);
+        sp = yp[m] + (double)(isb[m] ? b32[m].z : dp[m]);
+      } else {
+        su = isb[m] ? bv[m].x : yu[m];
+        sv = isb[m] ? bv[m].y : yv[m];
+        sp = isb[m] ? bv[m].z : yp[m];
+      }
+      qz[m] = M[m].x * su + M[m].z * sv;  // covProjPlane2Sphere, projection_mod.F90:79-96
+      qm[m] = M[m].y * su + M[m].w * sv;
       qp[m] = sp;
     }
     zw = ghost_interp<D>(qz, cc.x, cc.y, a.dx, a.dx2, a.dx3);
@@ -184,19 +224,15 @@ __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloA
     return;
   }
   // back to this panel's covariant winds (covProjSphere2Plane, :459-492)
-  const double4 N = a.Ntab[((p * 4 + e) * (H + 1) + h) * n + k];
-  int di, dj;
-  strip_point(e, -h, k, n, di, dj);
-  const long long o = mb + p * g.plane + (long long)(dj + H) * g.P + (di + H);
   const double uo = N.x * zw + N.z * mw, vo = N.y * zw + N.w * mw;
   if constexpr (!MIXED) {
     a.u[o] = uo;
     a.v[o] = vo;
     a.phi[o] = ph;
   } else {
-    a.du[o] = (float)(uo - a.u[o]);
-    a.dv[o] = (float)(vo - a.v[o]);
-    a.dp[o] = (float)(ph - a.phi[o]);
+    a.du[o] = (float)(uo - yu_d);
+    a.dv[o] = (float)(vo - yv_d);
+    a.dp[o] = (float)(ph - yp_d);
   }
 }
 
