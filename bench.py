@@ -249,7 +249,7 @@ def time_path(args, st, geom, precision, world, barrier, dist, local):
     cands, chosen = s.tuning()
     out = {"value": value, "ms_per_step": ms / args.steps, "stage_ms": stage_ms, "halo_ms": halo_ms,
            "achieved_gbs": achieved, "bytes_per_pv_step": sum(per_pv), "clocks": clk,
-           "tile": {"shape_fields": ["cells_x", "cells_y", "threads", "line_walks", "ctas_per_sm"],
+           "tile": {"shape_fields": ["cells_x", "cells_y", "threads", "walk_cells", "ctas_per_sm", "tma"],
                     "chosen": list(cands[chosen][0]),
                     "candidates": [{"shape": list(c), "ms": round(t, 5)} for c, t in cands]}}
     return s, out

@@ -129,8 +129,9 @@ int mcv_profile_step(mcv_handle *h, int nsteps, double *stage_ms, double *halo_m
 
 /* Stage-kernel tile shapes the autotuner timed on this handle's grid (it runs
  * once, before the first step): ncand (at most 16) candidates,
- * shapes[5*i..] = {cells in x, cells in y, threads, sweep style (0 per-cell
- * items, n walks of n cells), CTAs per SM the kernel's registers allow}, ms[i] =
+ * shapes[6*i..] = {cells in x, cells in y, threads, sweep style (0 per-cell
+ * items, n walks of n cells), CTAs per SM the kernel's registers allow, form
+ * (0 one CTA per tile, 1 persistent CTAs with TMA-staged tiles)}, ms[i] =
  * device time per launch, *chosen = the index in use.  No counterpart in the
  * reference (which has no GPU path). */
 int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, float *ms);

@@ -325,13 +325,13 @@ class Stepper:
         return list(st)[:nst], ha.value
 
     def tuning(self):
-        """Autotuner record: list of ((cells_x, cells_y, threads, walk, ctas_per_sm), ms per launch)
+        """Autotuner record: list of ((cells_x, cells_y, threads, walk, ctas_per_sm, tma), ms per launch)
         and the chosen index."""
         n, ch = ctypes.c_int(), ctypes.c_int()
-        shapes = (ctypes.c_int * 80)()
+        shapes = (ctypes.c_int * 96)()
         ms = (ctypes.c_float * 16)()
         _check(lib().mcv_tuning(self.h, ctypes.byref(n), ctypes.byref(ch), shapes, ms))
-        cands = [(tuple(shapes[5 * i: 5 * i + 5]), ms[i]) for i in range(n.value)]
+        cands = [(tuple(shapes[6 * i: 6 * i + 6]), ms[i]) for i in range(n.value)]
         return cands, ch.value
 
     def select_tile(self, index):

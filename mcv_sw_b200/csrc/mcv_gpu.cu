@@ -1075,11 +1075,12 @@ extern "C" int mcv_tuning(mcv_handle *h, int *ncand, int *chosen, int *shapes, f
   if (chosen) *chosen = h->choice;
   for (int i = 0; i < h->ncands; ++i) {
     if (shapes) {
-      shapes[5 * i] = h->cands[i].CX;
-      shapes[5 * i + 1] = h->cands[i].CY;
-      shapes[5 * i + 2] = h->cands[i].NT;
-      shapes[5 * i + 3] = h->cands[i].walk;
-      shapes[5 * i + 4] = h->cands[i].minb;
+      shapes[6 * i] = h->cands[i].CX;
+      shapes[6 * i + 1] = h->cands[i].CY;
+      shapes[6 * i + 2] = h->cands[i].NT;
+      shapes[6 * i + 3] = h->cands[i].walk;
+      shapes[6 * i + 4] = h->cands[i].minb;
+      shapes[6 * i + 5] = h->cands[i].tma ? 1 : 0;
     }
     if (ms) ms[i] = h->tune_ms[i];
   }
