@@ -524,6 +524,8 @@ __global__ void __launch_bounds__(NT, MINB)
   float *slope = reinterpret_cast<float *>(qref + 9);                  // [x, y][3]: derivative per radian
   uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + T::bar_off(MIXED));
   const int ntile = g.tiles_x * g.tiles_y;
+  // TMA form, loaded rows of 28..32 points: phase 0 maps lanes to columns
+  constexpr bool ROWMAP = TMA && LX >= 28 && LX <= 32 && NT % 32 == 0;
   // number of staged fields (split precision: the first stage has no input increment)
   constexpr int NF = MIXED ? (first_stage(KIND) ? 4 : 7) : 8;
 
@@ -684,7 +686,7 @@ __global__ void __launch_bounds__(NT, MINB)
 
   // one loaded point: r = {u, v, phi, phi_s, sqrtG, G^11, G^12, G^22} (FP64
   // policy) or {Y_u, Y_v, Y_phi} with f = {phi_s, d_u, d_v, d_phi} (split)
-  auto point = [&](int idx, int lx, int ly, const double *r, const float *f) {
+  auto point = [&](int idx, int lx, int ly, const double *r, const float *f, const double4 &mx, const double4 &my) {
     // interior points also keep sqrtG, cU, cV (and f) and form the interface
     // eigenvalues and upwind signs; split precision rounds those to FP32 here
     auto interior = [&](R sg, R cu, R cv, R fc, R g11, R g22, R phi) {
@@ -726,7 +728,7 @@ __global__ void __launch_bounds__(NT, MINB)
         p64 += (double)f[3];
       }
       MixPoint mp;
-      mix_point(mp, metx[lx], mety[ly], u64, v64, p64, (double)f[0], phibar, panel, a.two_omega);
+      mix_point(mp, mx, my, u64, v64, p64, (double)f[0], phibar, panel, a.two_omega);
       const double X = (double)(lx - H), Y = (double)(ly - H);
       const float e = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
       const float uu = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
@@ -754,12 +756,8 @@ __global__ void __launch_bounds__(NT, MINB)
     }
     parity ^= 1u;
     if constexpr (MIXED) make_planes();
-    for (int idx = threadIdx.x; idx < T::A; idx += NT) {
-      const int ly = idx / LX, lx = idx - ly * LX;
-      const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
-      if (lx >= lxe || ly >= lye || (xh && yh)) continue;  // tile corners are never read
-      double r[8];
-      float f[4];
+    // one staged point's input fields
+    auto staged = [&](int lx, int ly, double *r, float *f) {
       if constexpr (!MIXED) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) r[k] = stg64(k, lx, ly);
@@ -773,7 +771,35 @@ __global__ void __launch_bounds__(NT, MINB)
           f[3] = stg32(6, lx, ly);
         }
       }
-      point(idx, lx, ly, r, f);
+    };
+    if constexpr (ROWMAP) {
+      // lane = loaded column, warps stride over the rows: the column's halo
+      // flag, interface flags and metric entry are formed once per thread, and
+      // a warp reads one staged row (no bank conflicts across rows)
+      const int lx = threadIdx.x & 31;
+      if (lx < lxe) {
+        const bool xh = (lx < H) || (lx >= lxe - H);
+        const double4 mx = MIXED ? metx[lx] : double4{};
+        for (int ly = threadIdx.x >> 5; ly < lye; ly += NT / 32) {
+          const bool yh = (ly < H) || (ly >= lye - H);
+          if (xh && yh) continue;  // tile corners are never read
+          double r[8];
+          float f[4];
+          staged(lx, ly, r, f);
+          point(ly * LX + lx, lx, ly, r, f, mx, MIXED ? mety[ly] : mx);
+        }
+      }
+    } else {
+      for (int idx = threadIdx.x; idx < T::A; idx += NT) {
+        const int ly = idx / LX, lx = idx - ly * LX;
+        const bool xh = (lx < H) || (lx >= lxe - H), yh = (ly < H) || (ly >= lye - H);
+        if (lx >= lxe || ly >= lye || (xh && yh)) continue;  // tile corners are never read
+        double r[8];
+        float f[4];
+        staged(lx, ly, r, f);
+        const double4 zero{};
+        point(idx, lx, ly, r, f, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
+      }
     }
   } else {
     constexpr int CH = 3;  // points per thread whose loads are in flight together
@@ -833,7 +859,8 @@ __global__ void __launch_bounds__(NT, MINB)
         for (int j = 0; j < NL; ++j) rr[j] = r[j][k];
 #pragma unroll
         for (int j = 0; j < 4; ++j) ff[j] = f[j][k];
-        point(idx, lx, ly, rr, ff);
+        const double4 zero{};
+        point(idx, lx, ly, rr, ff, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
       }
     }
   }
