@@ -335,6 +335,35 @@ def stress_block(steps=200):
     return out
 
 
+def admission_block(order=4, nc=384, repeats=3):
+    """Admission of one new grid and request (the largest serving grid): the host
+    init chain (geometry build and upload, initial state on the host and
+    upload) vs geometry and initial state generated on the device.  Wall-clock
+    ms of the blocking API calls, best of `repeats`, handle creation excluded."""
+    import numpy as np
+    from mcv_sw_b200 import api, cases
+    times = {"host_chain": [], "device": []}
+    for _ in range(repeats):
+        for how in ("host_chain", "device"):
+            with api.Stepper(order, nc, 30.0, "RK3_TVD", precision="mixed", radius=cases.EARTH_RADIUS) as s:
+                t0 = time.perf_counter()
+                if how == "host_chain":
+                    geom = api.Geometry(order, nc, cases.EARTH_RADIUS)
+                    s.set_geometry(geom)
+                    spec = cases.balanced_flow_spec(geom, np.random.default_rng(17), lmax=8, rms=10.0, mountain=True)
+                    zw, mw, phi, phis = cases.balanced_flow_from_spec(geom, spec)
+                    u, v = api.sphere_to_cov(geom, zw, mw)
+                    s.set_member(0, phis, u, v, phi)
+                else:
+                    s.set_geometry_equiangular()
+                    spec = cases.balanced_flow_spec(s, np.random.default_rng(17), lmax=8, rms=10.0, mountain=True)
+                    s.set_member_balanced_flow(0, spec)
+                times[how].append(1e3 * (time.perf_counter() - t0))
+    return {"config": f"MCV{order} Nc={nc} split precision, balanced flow + degree<=8 harmonics + mountain",
+            "host_chain_ms": min(times["host_chain"]), "device_ms": min(times["device"]),
+            "speedup": min(times["host_chain"]) / min(times["device"])}
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -452,6 +481,7 @@ def run_ours(args):
             extra["serving"] = serving_block(args.serve_requests)
         if args.stress:
             extra["stress"] = stress_block()
+        extra["admission"] = admission_block()
     if rank == 0:
         other = "fp64" if args.precision == "mixed" else "mixed"
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -71,10 +71,41 @@ int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double *matrixG, 
                      const double *matrixA, const double *matrixIA, const double *f, const int *ghost_iref,
                      const double *ghost_coef);
 
+/* The same geometry computed on the device for the handle's (order, nc) and
+ * radius: the equiangular metric, the edge-strip matrices and the ghost
+ * weights that mcv_build_geometry + mcv_set_geometry produce, with no host
+ * arrays and no upload (new grids in a serving process).  Same formulas as
+ * mcv_build_geometry (src/projection_mod.F90:8-322, src/mesh_mod.F90:132-163,
+ * src/ghost_mod.f90:21-79); the device math library's tan/cos/atan2/pow
+ * differ from the host's by a few ulp. */
+int mcv_set_geometry_equiangular(mcv_handle *h);
+
+/* Copy the handle's metric back: sqrtG, G^11, G^12, G^22, f over the padded
+ * range (Fortran layout) and the ghost weights iref, coef as (nPVx, nPVHalo);
+ * any output may be NULL. */
+int mcv_get_geometry(mcv_handle *h, double *sqrtG, double *ig11, double *ig12, double *ig22, double *f,
+                     int *ghost_iref, double *ghost_coef);
+
 /* Upload member m's surface geopotential phi_s and its state: covariant u, v
  * and phi over the full padded range, halo included (the first stage of the
  * first step reads the caller's halo as src/time_scheme_mod.F90:27 does). */
 int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const double *u, const double *v, const double *phi);
+
+/* Member m's initial state generated on the device (no host arrays): the
+ * seeded balanced flow of the host init chain -- the tilted solid-body flow
+ * (gh0, u0, alpha; mcv_ic_tilted_zonal, src/test_case_mod.F90:118-120),
+ * plus g times the real spherical harmonics of degrees 1..lmax with the
+ * (lmax+1)^2 coefficients coef (mcv_ic_add_harmonics' ordering) rescaled to
+ * the area-weighted RMS height rms in metres (weightsOnPV x sqrtG quadrature),
+ * plus, if mountain_h0 > 0, the Gaussian mountain of height mountain_h0 m and
+ * e-folding distance efold m centred at (lon_c, lat_c) (mcv_ic_add_mountain),
+ * with the winds converted to covariant components (mcv_sphere_to_cov).
+ * Replaces mcv_set_member for this member; needs the geometry first.  The
+ * device math library and the order of the sums differ from the host chain's
+ * by a few ulp. */
+int mcv_set_member_balanced_flow(mcv_handle *h, int m, double gh0, double u0, double alpha, int lmax,
+                                 const double *coef, double rms, double mountain_h0, double lon_c, double lat_c,
+                                 double efold);
 
 /* Replace member m's state (u, v, phi over the padded range) and keep its
  * phi_s: the per-step input of a driver that owns the state on the host.

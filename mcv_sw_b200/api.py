@@ -52,6 +52,12 @@ def lib():
         "mcv_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_int, ctypes.POINTER(vp)]),
         "mcv_set_geometry": (ctypes.c_int, [vp, _D, _D, _D, _D, _D, _D, _I, _D]),
+        "mcv_set_geometry_equiangular": (ctypes.c_int, [vp]),
+        "mcv_get_geometry": (ctypes.c_int, [vp, _D, _D, _D, _D, _D, _I, _D]),
+        "mcv_set_member_balanced_flow": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_double, ctypes.c_int, _D, ctypes.c_double,
+                                                        ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_double]),
         "mcv_set_member": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
         "mcv_set_state": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D]),
         "mcv_step": (ctypes.c_int, [vp, ctypes.c_int]),
@@ -236,7 +242,7 @@ class Stepper:
 
     def __init__(self, order, nc, dt, scheme="RK3_TVD", members=1, precision="fp64", radius=6371220.0):
         self.order, self.nc, self.dt, self.scheme = int(order), int(nc), float(dt), scheme
-        self.members, self.precision = int(members), precision
+        self.members, self.precision, self.radius = int(members), precision, float(radius)
         self.npx, self.n, self.H = grid_sizes(order, nc)
         h = ctypes.c_void_p()
         _check(lib().mcv_create(self.order, self.nc, SCHEMES[scheme], PRECISIONS[precision], self.dt, float(radius),
@@ -264,6 +270,32 @@ class Stepper:
         _check(lib().mcv_set_geometry(self.h, _dp(geom.sqrtG), _dp(geom.matrixG), _dp(geom.matrixIG),
                                       _dp(geom.matrixA), _dp(geom.matrixIA), _dp(geom.f), _ip(geom.ghost_iref),
                                       _dp(geom.ghost_coef)))
+
+    def set_geometry_equiangular(self):
+        """Compute the grid geometry on the device (no host arrays, no upload)."""
+        _check(lib().mcv_set_geometry_equiangular(self.h))
+
+    def get_geometry(self):
+        """The handle's metric planes (padded, Fortran layout) and ghost weights."""
+        shp = (6, self.npx, self.npx)
+        out = {k: np.empty(shp) for k in ("sqrtG", "ig11", "ig12", "ig22", "f")}
+        nh = (self.order - 1, self.npx - 2 * (self.order - 1))
+        out["ghost_iref"] = np.empty(nh, dtype=np.int32)
+        out["ghost_coef"] = np.empty(nh)
+        _check(lib().mcv_get_geometry(self.h, *[_dp(out[k]) for k in ("sqrtG", "ig11", "ig12", "ig22", "f")],
+                                      _ip(out["ghost_iref"]), _dp(out["ghost_coef"])))
+        return out
+
+    def set_member_balanced_flow(self, m, spec):
+        """Member m's initial state generated on the device from a balanced-flow
+        spec (cases.balanced_flow_spec): no host arrays, no upload."""
+        lmax = int(spec["lmax"])
+        coef = np.ascontiguousarray(spec["coef"], dtype=np.float64) if lmax else None
+        mt = spec.get("mountain")
+        _check(lib().mcv_set_member_balanced_flow(
+            self.h, int(m), float(spec["gh0"]), float(spec["u0"]), float(spec["alpha"]), lmax, _dp(coef),
+            float(spec["rms"]), float(mt["h0"]) if mt else 0.0, float(mt["lon"]) if mt else 0.0,
+            float(mt["lat"]) if mt else 0.0, float(mt["efold"]) if mt else 1.0))
 
     def set_member(self, m, phi_s, u, v, phi):
         arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (phi_s, u, v, phi)]

@@ -11,8 +11,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 SOURCES = ["mcv_gpu.cu", "stage_d3_f64.cu", "stage_d3_mix.cu", "stage_d4_f64.cu", "stage_d4_mix.cu",
-           "mcv_noalloc.cu", "host_setup.cpp"]
-HEADERS = ["mcv_stage.cuh", "mcv_halo.cuh", "mcv_internal.h", os.path.join("..", "..", "include", "mcv_gpu.h")]
+           "mcv_geometry.cu", "mcv_noalloc.cu", "host_setup.cpp"]
+# per-source flags: the device geometry restates host formulas compiled
+# without FMA contraction
+SOURCE_FLAGS = {"mcv_geometry.cu": ["-fmad=false"]}
+HEADERS = ["mcv_stage.cuh", "mcv_halo.cuh", "mcv_tma.cuh", "mcv_ksum.cuh", "mcv_internal.h", os.path.join("..", "..", "include", "mcv_gpu.h")]
 OBJ_DIR = os.path.join(HERE, "_lib", "obj")
 
 NVCC_FLAGS = [
@@ -41,7 +44,8 @@ def build(force=False, verbose=False, extra_flags=()):
     for src in SOURCES:
         obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
-        cmd = [NVCC] + NVCC_FLAGS + list(extra_flags) + ["-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [NVCC] + NVCC_FLAGS + SOURCE_FLAGS.get(src, []) + list(extra_flags) + ["-c", os.path.join(CSRC, src),
+                                                                                    "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((src, subprocess.Popen(cmd)))

@@ -54,16 +54,6 @@ def area_rms(geom, h):
     return float(np.sqrt(np.sum(w * h * h) / np.sum(w)))
 
 
-def harmonic_height(geom, rng, lmin, lmax, rms):
-    """Random real spherical harmonics of degree lmin..lmax with Gaussian
-    coefficients, rescaled to the area-weighted RMS `rms` (metres)."""
-    coef = rng.standard_normal((lmax + 1) ** 2)
-    coef[: lmin * lmin] = 0.0
-    h = np.zeros(geom.shape)
-    api.add_harmonics(geom, h, coef, 1.0)
-    return h * (rms / area_rms(geom, h))
-
-
 def cfl_dt(geom, u, v, phi, cfl=0.5):
     """dt = cfl * (dx/(D-1)) / max over interior PVs of the two directions'
     signal speeds summed, (|c^1| + sqrt(G^11 phi)) + (|c^2| + sqrt(G^22 phi)):
@@ -102,12 +92,17 @@ def equator_gh0(u0, radius=EARTH_RADIUS, mean=GH0):
     return mean + (radius * 7.292e-5 * u0 + 0.5 * u0 * u0) / 3.0
 
 
-def balanced_flow(geom, rng, u0=38.6, alpha=0.05, lmax=8, rms=10.0, mountain=False, lmin=1):
-    zw, mw, phi = api.tilted_zonal(geom, equator_gh0(u0, geom.radius), u0, alpha)
-    phis = np.zeros(geom.shape)
+def balanced_flow_spec(geom, rng, u0=38.6, alpha=0.05, lmax=8, rms=10.0, mountain=False, lmin=1):
+    """The seeded parameters of a balanced flow, drawn from rng in a fixed order
+    (harmonic coefficients, then the mountain centre): what the host chain
+    (balanced_flow_from_spec) and the device generator
+    (Stepper.set_member_balanced_flow) build the same state from."""
+    spec = {"gh0": equator_gh0(u0, geom.radius), "u0": u0, "alpha": alpha, "lmax": int(lmax), "rms": rms,
+            "coef": None, "mountain": None}
     if lmax:
-        phi += GRAVITY * harmonic_height(geom, rng, lmin, lmax, rms)
-    meta = {"u0": u0, "alpha": alpha, "lmax": lmax, "rms_m": rms}
+        coef = rng.standard_normal((lmax + 1) ** 2)
+        coef[: lmin * lmin] = 0.0
+        spec["coef"] = coef
     if mountain:
         # summit uniform in longitude and in sin(latitude) within +-20 degrees:
         # with the ~3000 m mean depth (gh0 = 2.94e4) the balanced flow lowers the
@@ -115,8 +110,30 @@ def balanced_flow(geom, rng, u0=38.6, alpha=0.05, lmax=8, rms=10.0, mountain=Fal
         # it (phi -> 0, sqrt(G^ii phi) undefined) in the reference scheme as well
         lon_c = rng.uniform(0.0, 2.0 * np.pi)
         lat_c = float(np.arcsin(rng.uniform(-np.sin(np.radians(20.0)), np.sin(np.radians(20.0)))))
-        api.add_mountain(geom, phi, phis, lon_c, lat_c, 2000.0, 1.0e6)
-        meta.update(mountain_lon=lon_c, mountain_lat=lat_c)
+        spec["mountain"] = {"h0": 2000.0, "efold": 1.0e6, "lon": lon_c, "lat": lat_c}
+    return spec
+
+
+def balanced_flow_from_spec(geom, spec):
+    """Host arrays (zonal, meridional, phi, phi_s) of a balanced-flow spec."""
+    zw, mw, phi = api.tilted_zonal(geom, spec["gh0"], spec["u0"], spec["alpha"])
+    phis = np.zeros(geom.shape)
+    if spec["lmax"]:
+        h = np.zeros(geom.shape)
+        api.add_harmonics(geom, h, spec["coef"], 1.0)
+        phi += GRAVITY * (h * (spec["rms"] / area_rms(geom, h)))
+    mt = spec["mountain"]
+    if mt:
+        api.add_mountain(geom, phi, phis, mt["lon"], mt["lat"], mt["h0"], mt["efold"])
+    return zw, mw, phi, phis
+
+
+def balanced_flow(geom, rng, u0=38.6, alpha=0.05, lmax=8, rms=10.0, mountain=False, lmin=1):
+    spec = balanced_flow_spec(geom, rng, u0, alpha, lmax, rms, mountain, lmin)
+    zw, mw, phi, phis = balanced_flow_from_spec(geom, spec)
+    meta = {"u0": u0, "alpha": alpha, "lmax": lmax, "rms_m": rms}
+    if spec["mountain"]:
+        meta.update(mountain_lon=spec["mountain"]["lon"], mountain_lat=spec["mountain"]["lat"])
     return zw, mw, phi, phis, meta
 
 

@@ -774,6 +774,69 @@ extern "C" int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double
   return MCV_OK;
 }
 
+extern "C" int mcv_set_geometry_equiangular(mcv_handle *h) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (!(h->radius > 0.)) return fail(MCV_ERR_ARG, "the handle's radius must be positive");
+  const double pi = 2.0 * std::asin(1.0);
+  GeomArgs a{};
+  a.order = h->order;
+  a.nc = h->nc;
+  a.npx = h->npx;
+  a.n = h->g.n;
+  a.H = h->H;
+  a.P = h->g.P;
+  a.radius = h->radius;
+  a.dx = h->g.dx;  // (90 / nc) degrees in radians, as the host builder
+  a.x_min = -45. * (pi / 180.);
+  a.pi = pi;
+  a.sqrtG = h->sqrtG;
+  a.ig11 = h->ig11;
+  a.ig12 = h->ig12;
+  a.ig22 = h->ig22;
+  a.fcor = h->fcor;
+  a.Mtab = h->Mtab;
+  a.Ntab = h->Ntab;
+  a.giref = h->giref;
+  a.gcoef = h->gcoef;
+  a.met1d = h->mixed ? h->met1d : nullptr;
+  a.err = h->err;
+  MCV_CUDA(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "clear error flag");
+  if (int e = build_geometry_device(a, h->stream))
+    return fail(MCV_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+  int bad = 0;
+  MCV_CUDA(cudaMemcpyAsync(&bad, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "read error flag");
+  MCV_CUDA(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "clear error flag");
+  const size_t NP = (size_t)h->npx * h->npx * 6;
+  h->sqrtG_host.resize(NP);
+  if (int rc = download_padded(h, h->sqrtG_host.data(), h->sqrtG)) return rc;
+  MCV_CUDA(cudaStreamSynchronize(h->stream), "device geometry");
+  if (bad) return fail(MCV_ERR_ARG, "ghost cell location error");
+  h->geometry_set = true;
+  return MCV_OK;
+}
+
+extern "C" int mcv_get_geometry(mcv_handle *h, double *sqrtG, double *ig11, double *ig12, double *ig22, double *f,
+                                int *ghost_iref, double *ghost_coef) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (!h->geometry_set) return fail(MCV_ERR_ORDER, "no geometry set");
+  int rc;
+  const double *src[5] = {h->sqrtG, h->ig11, h->ig12, h->ig22, h->fcor};
+  double *dst[5] = {sqrtG, ig11, ig12, ig22, f};
+  for (int k = 0; k < 5; ++k)
+    if (dst[k] && (rc = download_padded(h, dst[k], src[k]))) return rc;
+  const size_t nh = (size_t)h->H * h->g.n;
+  std::vector<double2> coef(ghost_coef ? nh : 0);
+  if (ghost_iref)
+    MCV_CUDA(cudaMemcpyAsync(ghost_iref, h->giref, sizeof(int) * nh, cudaMemcpyDeviceToHost, h->stream),
+             "download iref");
+  if (ghost_coef)
+    MCV_CUDA(cudaMemcpyAsync(coef.data(), h->gcoef, sizeof(double2) * nh, cudaMemcpyDeviceToHost, h->stream),
+             "download coef");
+  MCV_CUDA(cudaStreamSynchronize(h->stream), "download geometry");
+  for (size_t k = 0; k < coef.size(); ++k) ghost_coef[k] = coef[k].x;
+  return MCV_OK;
+}
+
 extern "C" int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const double *u, const double *v,
                               const double *phi) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
@@ -809,6 +872,116 @@ extern "C" int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const d
              "upload mean depth");
   }
   MCV_CUDA(cudaStreamSynchronize(h->stream), "member upload");
+  h->member_set[m] = 1;
+  h->steps_done[m] = 0;
+  return MCV_OK;
+}
+
+namespace {
+
+// Compensated total of the per-block partial sums {s1, c1, s2, c2} (fixed
+// order: the same bits on every call).
+int sum_partials(mcv_handle *h, double &s1, double &s2) {
+  std::vector<double4> part(kPartialBlocks);
+  MCV_CUDA(cudaMemcpyAsync(part.data(), h->partial, sizeof(double4) * kPartialBlocks, cudaMemcpyDeviceToHost,
+                           h->stream),
+           "download partial sums");
+  MCV_CUDA(cudaStreamSynchronize(h->stream), "partial sums");
+  KSum a{0., 0.}, b{0., 0.};
+  auto add = [](KSum &k, double x) {
+    const double t = k.s + x;
+    if (std::fabs(k.s) >= std::fabs(x)) k.c += (k.s - t) + x;
+    else k.c += (x - t) + k.s;
+    k.s = t;
+  };
+  for (const double4 &q : part) {
+    add(a, q.x);
+    a.c += q.y;
+    add(b, q.z);
+    b.c += q.w;
+  }
+  s1 = a.s + a.c;
+  s2 = b.s + b.c;
+  return MCV_OK;
+}
+
+}  // namespace
+
+extern "C" int mcv_set_member_balanced_flow(mcv_handle *h, int m, double gh0, double u0, double alpha, int lmax,
+                                            const double *coef, double rms, double mountain_h0, double lon_c,
+                                            double lat_c, double efold) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (m < 0 || m >= h->members) return fail(MCV_ERR_ARG, "member index out of range");
+  if (!h->geometry_set) return fail(MCV_ERR_ORDER, "the geometry must precede the member's initial state");
+  if (lmax < 0 || lmax > 200 || (lmax > 0 && !coef)) return fail(MCV_ERR_ARG, "bad harmonic arguments");
+  if (mountain_h0 > 0. && !(efold > 0.)) return fail(MCV_ERR_ARG, "bad mountain arguments");
+  const long long off = (long long)m * h->g.mstride;
+  if (h->mixed) h->mcur[m] = h->cur;
+  double *const *Y = state(h, m);
+  const double pi = 2.0 * std::asin(1.0);
+  IcArgs a{};
+  a.order = h->order;
+  a.nc = h->nc;
+  a.npx = h->npx;
+  a.n = h->g.n;
+  a.H = h->H;
+  a.P = h->g.P;
+  a.radius = h->radius;
+  a.dx = h->g.dx;
+  a.x_min = -45. * (pi / 180.);
+  a.pi = pi;
+  a.gh0 = gh0;
+  a.u0 = u0;
+  a.alpha = alpha;
+  a.mountain = mountain_h0 > 0.;
+  a.h0 = mountain_h0;
+  a.lon_c = lon_c;
+  a.lat_c = lat_c;
+  a.efold = efold;
+  a.u = Y[0] + off;
+  a.v = Y[1] + off;
+  a.phi = Y[2] + off;
+  a.phis = h->phis + off;
+  a.phis32 = h->mixed ? h->phis32 + off : nullptr;
+  a.sqrtG = h->sqrtG;
+  double *dcoef = nullptr;
+  int rc;
+  if (lmax > 0 && rms != 0.) {
+    const size_t nb = sizeof(double) * (size_t)(lmax + 1) * (lmax + 1);
+    MCV_CUDA(cudaMallocAsync((void **)&dcoef, nb, h->stream), "coefficients");
+    MCV_CUDA(cudaMemcpyAsync(dcoef, coef, nb, cudaMemcpyHostToDevice, h->stream), "upload coefficients");
+    a.coef = dcoef;
+    a.lmax = lmax;
+    // unit-scale height, then its area-weighted RMS (cases.harmonic_height)
+    int e = ic_harmonics_device(a, h->stream);
+    if (!e) e = ic_sums_device(a, 0, a.phis, h->partial, kPartialBlocks, h->stream);
+    if (e) {
+      cudaFreeAsync(dcoef, h->stream);
+      return fail(MCV_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+    }
+    double swh2 = 0., sw = 0.;
+    if ((rc = sum_partials(h, swh2, sw))) return rc;
+    const double area_rms = std::sqrt(swh2 / sw);
+    if (!(area_rms > 0.)) {
+      cudaFreeAsync(dcoef, h->stream);
+      return fail(MCV_ERR_ARG, "the harmonic coefficients give a zero field");
+    }
+    a.ratio = rms / area_rms;
+  }
+  int e = ic_fields_device(a, h->stream);
+  if (dcoef) cudaFreeAsync(dcoef, h->stream);
+  if (e) return fail(MCV_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+  if (h->mixed) {
+    // mean depth: sqrtG-weighted mean of phi over the interior points
+    if ((e = ic_sums_device(a, 1, a.phi, h->partial, kPartialBlocks, h->stream)))
+      return fail(MCV_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+    double num = 0., den = 0.;
+    if ((rc = sum_partials(h, num, den))) return rc;
+    h->phibar_host[m] = num / den;
+    MCV_CUDA(cudaMemcpyAsync(h->phibar + m, &h->phibar_host[m], sizeof(double), cudaMemcpyHostToDevice, h->stream),
+             "upload mean depth");
+  }
+  MCV_CUDA(cudaStreamSynchronize(h->stream), "member initial state");
   h->member_set[m] = 1;
   h->steps_done[m] = 0;
   return MCV_OK;

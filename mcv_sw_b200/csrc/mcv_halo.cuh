@@ -1,5 +1,6 @@
 // mcv_halo.cuh -- halo/boundary kernel (K2) and diagnostics of MCV_SW.
 #pragma once
+#include "mcv_ksum.cuh"
 #include "mcv_stage.cuh"
 
 namespace mcv {
@@ -240,19 +241,6 @@ __global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloA
 // Mass / energy (src/diag_mod.F90:10-67): per-cell sums in the reference's
 // order, then a compensated (Neumaier) sum over cells.
 // ---------------------------------------------------------------------------
-struct KSum {
-  double s, c;
-};
-__device__ __forceinline__ void neumaier_add(KSum &a, double x) {
-  const double t = a.s + x;
-  if (fabs(a.s) >= fabs(x)) a.c += (a.s - t) + x;
-  else a.c += (x - t) + a.s;
-  a.s = t;
-}
-__device__ __forceinline__ void ksum_merge(KSum &a, const KSum &b) {
-  neumaier_add(a, b.s);
-  a.c += b.c;
-}
 
 template <int D>
 __global__ void __launch_bounds__(256) mass_energy_kernel(const GridDesc g, const double *u, const double *v,
