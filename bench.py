@@ -47,6 +47,7 @@ def parse_args():
     p.add_argument("--ensemble", type=int, default=1, help="run the 64-member ensemble block (1 GPU only)")
     p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving block (0: skip)")
     p.add_argument("--stress", type=int, default=1, help="run the Nc=1024 roofline-stress block (1 GPU only)")
+    p.add_argument("--admission", type=int, default=1, help="run the device-admission timing block (1 GPU only)")
     p.add_argument("--tiles", default=None,
                    help="pin the stage-kernel candidates of the main workload as 'fp64_index,mixed_index' "
                         "(default: each handle's autotuner chooses)")
@@ -481,7 +482,8 @@ def run_ours(args):
             extra["serving"] = serving_block(args.serve_requests)
         if args.stress:
             extra["stress"] = stress_block()
-        extra["admission"] = admission_block()
+        if args.admission:
+            extra["admission"] = admission_block()
     if rank == 0:
         other = "fp64" if args.precision == "mixed" else "mixed"
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
