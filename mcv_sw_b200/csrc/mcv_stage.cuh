@@ -568,6 +568,9 @@ __global__ void __launch_bounds__(NT, MINB)
       bulk_load(metx + LX, a.met1d + Y0, (uint32_t)ny * sizeof(double4), bar);
     }
   };
+  // 1 / (full tile width in radians), x and y (split precision's linear references)
+  const double2 inv_full_w = MIXED ? make_double2(1. / ((double)CX * g.dx), 1. / ((double)CY * g.dx))
+                                   : make_double2(0., 0.);
   uint32_t parity = 0;
   if constexpr (TMA) {
     if (threadIdx.x == 0) {
@@ -684,6 +687,48 @@ __global__ void __launch_bounds__(NT, MINB)
     __syncthreads();
   };
 
+  // TMA form, split precision: make_planes from the staged tile, by warp 0
+  // alone and without block barriers (the caller's barrier publishes it).
+  // The widths' reciprocals replace the division (the slopes are rounded to
+  // FP32 anyway and the plane takes its slope from the rounded value).
+  auto fit_planes_warp0 = [&]() {
+    const int lane = threadIdx.x;
+    double q[3] = {0., 0., 0.};
+    if (lane < 3) {
+      const int lx = H + (lane == 1 ? txe - 1 : 0), ly = H + (lane == 2 ? tye - 1 : 0);
+      double u = stg64(0, lx, ly), v = stg64(1, lx, ly), p = stg64(2, lx, ly);
+      const double phs = (double)stg32(3, lx, ly);
+      if constexpr (!first_stage(KIND)) {
+        u += (double)stg32(4, lx, ly);
+        v += (double)stg32(5, lx, ly);
+        p += (double)stg32(6, lx, ly);
+      }
+      MixPoint mp;
+      mix_point(mp, metx[lx], mety[ly], u, v, p, phs, phibar, panel, a.two_omega);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) q[j] = mp.q[j];
+    }
+    double r[3][3];  // [reference point][quantity]
+#pragma unroll
+    for (int pnt = 0; pnt < 3; ++pnt)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) r[pnt][j] = __shfl_sync(0xffffffffu, q[j], pnt);
+    if (lane < 3) {
+      const double q0 = (lane == 0) ? r[0][0] : (lane == 1) ? r[0][1] : r[0][2];
+      const double qx = (lane == 0) ? r[1][0] : (lane == 1) ? r[1][1] : r[1][2];
+      const double qy = (lane == 0) ? r[2][0] : (lane == 1) ? r[2][1] : r[2][2];
+      const double iwx = (ncx == CX) ? inv_full_w.x : 1. / ((double)ncx * g.dx);
+      const double iwy = (ncy == CY) ? inv_full_w.y : 1. / ((double)ncy * g.dx);
+      const float sx = (float)((qx - q0) * iwx);
+      const float sy = (float)((qy - q0) * iwy);
+      plane[3 * lane] = q0;
+      plane[3 * lane + 1] = (double)sx * (g.dx / (double)(D - 1));  // per point index
+      plane[3 * lane + 2] = (double)sy * (g.dx / (double)(D - 1));
+      slope[lane] = sx;
+      slope[3 + lane] = sy;
+    }
+  };
+
   // one loaded point: r = {u, v, phi, phi_s, sqrtG, G^11, G^12, G^22} (FP64
   // policy) or {Y_u, Y_v, Y_phi} with f = {phi_s, d_u, d_v, d_phi} (split)
   auto point = [&](int idx, int lx, int ly, const double *r, const float *f, const double4 &mx, const double4 &my) {
@@ -748,14 +793,25 @@ __global__ void __launch_bounds__(NT, MINB)
 
   if constexpr (TMA) {
     // wait for this item's copies; every thread agrees before anyone leaves
-    const bool arrived = mbar_wait_bounded(bar, parity);
-    if (__syncthreads_or(!arrived)) {
+    bool bad;
+    if constexpr (MIXED) {
+      // warp 0 alone waits, then fits the linear references (lanes 0-2, values
+      // exchanged by shuffles); one block barrier publishes both
+      bool got = true;
+      if (threadIdx.x < 32) {
+        got = __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity));
+        if (got) fit_planes_warp0();
+      }
+      bad = __syncthreads_or(!got);
+    } else {
+      bad = __syncthreads_or(!mbar_wait_bounded(bar, parity));
+    }
+    if (bad) {
       if (threadIdx.x == 0) atomicExch(a.err, 1);
       mbar_wait_bounded(bar, parity);  // the copies in flight land before the CTA exits
       return;
     }
     parity ^= 1u;
-    if constexpr (MIXED) make_planes();
     // one staged point's input fields
     auto staged = [&](int lx, int ly, double *r, float *f) {
       if constexpr (!MIXED) {
