@@ -404,12 +404,14 @@ struct Tile {
   static constexpr int YR = XR + 3 * I;
   static constexpr int TOTAL = YR + 3 * I;
   // split precision, after the R arrays: 1-D metric tables [LX] and [LY] double4,
-  // then the per-tile linear references of E, u, v: planes [3][3] double,
-  // reference-point values [3][3] double, slopes [2][3] float
+  // then two buffers (alternate work items of the TMA form) of the per-tile
+  // linear references of E, u, v: planes [3][3] double, reference-point values
+  // [3][3] double, slopes [2][3] float
   static constexpr size_t MET_OFF = ((size_t)TOTAL * sizeof(R) + 31) / 32 * 32;
   static constexpr size_t PLANE_OFF = MET_OFF + (size_t)(LX + LY) * sizeof(double4);
+  static constexpr size_t PLANE_BYTES = 176;  // 18 doubles + 6 floats, a 16-byte multiple
   __host__ __device__ static constexpr size_t bytes(bool mixed) {
-    return mixed ? PLANE_OFF + 18 * sizeof(double) + 6 * sizeof(float) : (size_t)TOTAL * sizeof(R);
+    return mixed ? PLANE_OFF + 2 * PLANE_BYTES : (size_t)TOTAL * sizeof(R);
   }
   // TMA form, after all of the above: one work item's input fields as staged
   // boxes [LY][BX] (FP64 policy: 8 FP64 fields; split precision: 3 FP64 then 4
@@ -522,6 +524,7 @@ __global__ void __launch_bounds__(NT, MINB)
   double *plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF);  // [3] {value at (H, H), d/dlx, d/dly}
   double *qref = plane + 9;                                            // [3 points][3]
   float *slope = reinterpret_cast<float *>(qref + 9);                  // [x, y][3]: derivative per radian
+  int pb = 0;  // TMA form: plane buffer of the current work item
   uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + T::bar_off(MIXED));
   const int ntile = g.tiles_x * g.tiles_y;
   // TMA form, loaded rows of 28..32 points: phase 0 maps lanes to columns
@@ -582,6 +585,14 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   const int wfirst = TMA ? (int)blockIdx.x : 0, wstep = TMA ? (int)gridDim.x : 1, wend = TMA ? tm.total : 1;
   for (int wi = wfirst; wi < wend; wi += wstep) {
+  if constexpr (TMA && MIXED) {
+    // alternate buffers: warp 0 fits the next item's references while the
+    // other warps may still read this item's slopes in phase A
+    plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF + pb * T::PLANE_BYTES);
+    qref = plane + 9;
+    slope = reinterpret_cast<float *>(qref + 9);
+    pb ^= 1;
+  }
   int tx, ty, panel, mem;
   if constexpr (TMA) {
     const WorkItem item = decode_item(wi, g.tiles_x, g.tiles_y, nslots);
@@ -1302,7 +1313,9 @@ __global__ void __launch_bounds__(NT, MINB)
     }
   }
   }
-  if constexpr (TMA) __syncthreads();  // the next item reuses the shared arrays
+  // (TMA form: no barrier here.  The next item writes the shared arrays only
+  // after its own first block barrier, which every thread reaches after this
+  // item's phase A; before it, warp 0 writes only the other plane buffer.)
   }
 }
 
