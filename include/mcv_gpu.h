@@ -139,6 +139,15 @@ int mcv_set_active(mcv_handle *h, int count, const int *members);
  * Inf, else 0.  Returns MCV_ERR_NONFINITE if an active member is flagged. */
 int mcv_check_finite(mcv_handle *h, int *flags);
 
+/* Failure-path check, with no GPU fault, of the bounded wait the stage kernels
+ * use on their staged copies (no reference counterpart): one warp waits on a
+ * fresh mbarrier that nothing completes (complete = 0) or that is completed
+ * first (complete = 1), giving up after limit_ms (0 < limit_ms <= 2000).
+ * *timed_out = 1 if the wait gave up; *elapsed_ms = the wait's device time.
+ * The stage kernels wait with a limit of about one second, then raise the flag
+ * mcv_sync reports and return. */
+int mcv_selftest_wait(int complete, double limit_ms, int *timed_out, double *elapsed_ms);
+
 /* Download member m's state over the padded range (any pointer may be NULL).
  * phiG = phi * sqrtG as src/time_scheme_mod.F90:85 stores it. */
 int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double *phi, double *phiG);

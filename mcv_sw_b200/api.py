@@ -66,6 +66,7 @@ def lib():
         "mcv_query": (ctypes.c_int, [vp]),
         "mcv_set_active": (ctypes.c_int, [vp, ctypes.c_int, _I]),
         "mcv_check_finite": (ctypes.c_int, [vp, _I]),
+        "mcv_selftest_wait": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _I, _D]),
         "mcv_get_state": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
         "mcv_mass_energy": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
         "mcv_destroy": (ctypes.c_int, [vp]),
@@ -176,6 +177,14 @@ class Geometry:
         for c in range(self.nc):
             line[self.H + c * (D - 1): self.H + c * (D - 1) + D] += w1
         return np.broadcast_to(np.outer(line, line), self.shape)
+
+
+def selftest_wait(complete, limit_ms):
+    """Run the stage kernels' bounded copy wait on an mbarrier that is
+    (complete=True) or is never (False) completed: (timed_out, elapsed_ms)."""
+    t, ms = ctypes.c_int(), ctypes.c_double()
+    _check(lib().mcv_selftest_wait(int(bool(complete)), float(limit_ms), ctypes.byref(t), ctypes.byref(ms)))
+    return bool(t.value), ms.value
 
 
 # ---------------------------------------------------------------- initial conditions

@@ -1050,6 +1050,57 @@ extern "C" int mcv_sync(mcv_handle *h) {
   return MCV_OK;
 }
 
+namespace {
+
+// Failure path of the stage kernels' bounded copy wait (mbar_wait_bounded),
+// run without a GPU fault: one warp waits on a fresh mbarrier; with `complete`
+// thread 0 arrives first and the wait must succeed at once, otherwise nothing
+// ever arrives and the wait must give up after limit_ns and say so, as the
+// stage kernel does before it raises its error flag and returns.
+__global__ void wait_selftest_kernel(int complete, unsigned long long limit_ns, int *timed_out,
+                                     unsigned long long *elapsed_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (complete && threadIdx.x == 0) mbar_arrive(&bar);
+  __syncthreads();  // the arrival, if any, precedes every wait
+  const uint64_t t0 = global_ns();
+  const bool got = mbar_wait_bounded(&bar, 0u, limit_ns);
+  const uint64_t t1 = global_ns();
+  if (__syncthreads_or(!got) && threadIdx.x == 0) *timed_out = 1;
+  if (threadIdx.x == 0) *elapsed_ns = t1 - t0;
+}
+
+}  // namespace
+
+extern "C" int mcv_selftest_wait(int complete, double limit_ms, int *timed_out, double *elapsed_ms) {
+  if (!timed_out || !elapsed_ms) return fail(MCV_ERR_ARG, "output pointer is NULL");
+  if (!(limit_ms > 0.) || limit_ms > 2000.) return fail(MCV_ERR_ARG, "limit_ms must be in (0, 2000]");
+  struct Out {
+    int timed_out;
+    int pad;
+    unsigned long long elapsed_ns;
+  };
+  Out *d = nullptr;
+  MCV_CUDA(cudaMalloc((void **)&d, sizeof(Out)), "self-test buffer");
+  Out o{};
+  cudaError_t e = cudaMemset(d, 0, sizeof(Out));
+  if (e == cudaSuccess) {
+    wait_selftest_kernel<<<1, 32>>>(complete, (unsigned long long)(limit_ms * 1e6), &d->timed_out, &d->elapsed_ns);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&o, d, sizeof(Out), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "wait self-test");
+  *timed_out = o.timed_out;
+  *elapsed_ms = (double)o.elapsed_ns * 1e-6;
+  return MCV_OK;
+}
+
 extern "C" int mcv_query(mcv_handle *h) {
   if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
   const cudaError_t e = cudaStreamQuery(h->stream);

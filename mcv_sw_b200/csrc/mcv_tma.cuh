@@ -78,16 +78,21 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Bounded wait for phase `parity` of the barrier: gives up after about one
-// second of wall time (and at most 2^24 polls), far beyond the microseconds a
-// tile's copies take.  Returns false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Bounded wait for phase `parity` of the barrier: gives up after limit_ns of
+// wall time (default about one second, far beyond the microseconds a tile's
+// copies take) and at most 2^24 polls.  Returns false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint64_t limit_ns = 1000000000ull) {
   const uint64_t t0 = global_ns();
   for (int it = 0; it < (1 << 24); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (global_ns() - t0 > 1000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
   return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 }  // namespace mcv
