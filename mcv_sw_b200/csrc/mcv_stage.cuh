@@ -648,33 +648,18 @@ __global__ void __launch_bounds__(NT, MINB)
     return reinterpret_cast<const float *>(smraw + T::field_off(MIXED, f))[ly * T::BX + lx];
   };
 
-  // split precision: the per-tile linear references (two block barriers)
+  // split precision, direct form: the per-tile linear references (two block barriers)
   auto make_planes = [&]() {
     if (threadIdx.x < 3) {
       // reference points (H, H), (txe - 1 + H, H), (H, tye - 1 + H): interior
       const int lx = H + (threadIdx.x == 1 ? txe - 1 : 0), ly = H + (threadIdx.x == 2 ? tye - 1 : 0);
-      double u, v, p, phs;
-      if constexpr (TMA) {
-        u = stg64(0, lx, ly);
-        v = stg64(1, lx, ly);
-        p = stg64(2, lx, ly);
-        phs = (double)stg32(3, lx, ly);
-        if constexpr (!first_stage(KIND)) {
-          u += (double)stg32(4, lx, ly);
-          v += (double)stg32(5, lx, ly);
-          p += (double)stg32(6, lx, ly);
-        }
-      } else {
-        const int o = ly * g.P + lx;
-        u = __ldg(t_yu + o);
-        v = __ldg(t_yv + o);
-        p = __ldg(t_yp + o);
-        phs = (double)__ldg(t_p32 + o);
-        if constexpr (!first_stage(KIND)) {
-          u += (double)__ldg(t_du + o);
-          v += (double)__ldg(t_dv + o);
-          p += (double)__ldg(t_dp + o);
-        }
+      const int o = ly * g.P + lx;
+      double u = __ldg(t_yu + o), v = __ldg(t_yv + o), p = __ldg(t_yp + o);
+      const double phs = (double)__ldg(t_p32 + o);
+      if constexpr (!first_stage(KIND)) {
+        u += (double)__ldg(t_du + o);
+        v += (double)__ldg(t_dv + o);
+        p += (double)__ldg(t_dp + o);
       }
       MixPoint mp;
       mix_point(mp, a.met1d[X0 + lx], a.met1d[Y0 + ly], u, v, p, phs, phibar, panel, a.two_omega);
