@@ -769,15 +769,21 @@ extern "C" int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double
     // 1-D metric table of the equiangular panel coordinate x_i = (i-1) dx/(D-1) + x_min
     // (mesh_mod.F90:135-136); the same table serves y because dx == dy.
     const double R = h->radius, D2R = (2.0 * std::asin(1.0)) / 180.;
-    const size_t centre = (size_t)(npx / 2) + (size_t)npx * (npx / 2);
-    if (std::fabs(sqrtG[centre] / (R * R) - 1.) > 1e-6)
-      return fail(MCV_ERR_ARG, "radius does not match the geometry's sqrtG (mixed precision recomputes the metric)");
     met.resize(npx);
     for (int i = 0; i < npx; ++i) {
       const double x = (double)(i + (1 - H) - 1) * h->g.dx / (double)(h->order - 1) + (-45. * D2R);
       const double t = std::tan(x), c = std::cos(x), s = std::sin(x);
       met[i] = make_double4(t, c * c / (R * R), s * c / R, R / (c * c));
     }
+    // the kernels recompute sqrtG from this table: it must be the caller's
+    // geometry (same radius), checked at the middle padded point of panel 1
+    const int mid = npx / 2;
+    const double4 mx = met[mid];
+    const double rho2 = 1. + mx.x * mx.x + mx.x * mx.x;
+    const double sg_table = mx.w * mx.w / (rho2 * std::sqrt(rho2));
+    const size_t k = (size_t)mid + (size_t)npx * mid;
+    if (std::fabs(sqrtG[k] / sg_table - 1.) > 1e-9)
+      return fail(MCV_ERR_ARG, "radius does not match the geometry's sqrtG (mixed precision recomputes the metric)");
   }
   int rc;
   if ((rc = upload_padded(h, h->sqrtG, sqrtG, 8))) return rc;

@@ -120,3 +120,16 @@ def test_every_shape_members_and_active_set(order):
             for k in ("u", "v", "phi"):
                 assert np.array_equal(idle[k], getattr(states[1], k)), (cands[i][0], k)
             s.set_active([0, 1, 2])
+
+
+@pytest.mark.parametrize("order,nc", [(4, 3), (4, 8), (3, 5)])
+def test_geometry_of_another_radius_is_rejected(order, nc):
+    """Split precision recomputes the metric from the handle's radius, so a
+    geometry built for another radius is refused; the matching one (panel
+    centre on a point or not) is accepted."""
+    geom = api.Geometry(order, nc, cases.EARTH_RADIUS)
+    with api.Stepper(order, nc, 60.0, "RK3_TVD", precision="mixed", radius=cases.EARTH_RADIUS) as s:
+        s.set_geometry(geom)
+    with api.Stepper(order, nc, 60.0, "RK3_TVD", precision="mixed", radius=0.99 * cases.EARTH_RADIUS) as s:
+        with pytest.raises(api.MCVError):
+            s.set_geometry(geom)
