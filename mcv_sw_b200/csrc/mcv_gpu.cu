@@ -124,6 +124,7 @@ struct mcv_handle {
   float4 *bnd32 = nullptr;
   double4 *met1d = nullptr;
   double *phibar = nullptr;
+  double *prec = nullptr;  // TMA form: per (member, panel, tile) linear references of a step's first stage
   std::vector<double> phibar_host;
   // shared
   double *sqrtG = nullptr, *ig11 = nullptr, *ig12 = nullptr, *ig22 = nullptr, *fcor = nullptr, *phis = nullptr;
@@ -173,7 +174,7 @@ struct Layout {
   size_t total = 0;
   size_t f64_state[9]{}, f64_acc[3]{}, mix_state[6]{}, mix_inc[6]{}, mix_acc[3]{};
   size_t metric[5]{}, phis = 0, phis32 = 0, bnd = 0, bnd32 = 0, M = 0, N = 0, iref = 0, coef = 0, partial = 0,
-         met1d = 0, phibar = 0, active = 0, flags = 0, err = 0, stage = 0;
+         met1d = 0, phibar = 0, active = 0, flags = 0, err = 0, stage = 0, prec = 0;
 };
 
 Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int members) {
@@ -201,6 +202,12 @@ Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int memb
     L.bnd32 = take(sizeof(float4) * 24 * (size_t)g.n * members);
     L.met1d = take(sizeof(double4) * (size_t)g.np);
     L.phibar = take(sizeof(double) * members);
+    // 96-byte linear-reference records for the most tiles any candidate shape makes
+    int ncand = 0, most = 0;
+    const StageLauncher *cands = stage_launchers(H + 1, true, &ncand);
+    for (int c = 0; c < ncand; ++c)
+      most = std::max(most, ((g.Nc + cands[c].CX - 1) / cands[c].CX) * ((g.Nc + cands[c].CY - 1) / cands[c].CY));
+    L.prec = take((size_t)96 * 6 * most * members);
   }
   for (int k = 0; k < 5; ++k) L.metric[k] = take(plane6);
   L.phis = take(f64);
@@ -302,7 +309,7 @@ StageArgs stage_args(mcv_handle *h, int s, int c) {
   a.yu = Y[0]; a.yv = Y[1]; a.yp = Y[2];
   a.uo = Yn[0]; a.vo = Yn[1]; a.po = Yn[2];
   a.fU = h->facc[0]; a.fV = h->facc[1]; a.fP = h->facc[2];
-  a.phis32 = h->phis32; a.met1d = h->met1d; a.phibar = h->phibar; a.bnd32 = h->bnd32;
+  a.phis32 = h->phis32; a.met1d = h->met1d; a.phibar = h->phibar; a.bnd32 = h->bnd32; a.prec = h->prec;
   a.two_omega = 2. * kOmega;
   float *const *din = nullptr, *const *dout = nullptr;
   float wd = 0.f, wt = 0.f;
@@ -670,6 +677,7 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
     h->bnd32 = (float4 *)(base + L.bnd32);
     h->met1d = (double4 *)(base + L.met1d);
     h->phibar = (double *)(base + L.phibar);
+    h->prec = (double *)(base + L.prec);
   }
   h->sqrtG = (double *)(base + L.metric[0]);
   h->ig11 = (double *)(base + L.metric[1]);

@@ -75,6 +75,7 @@ struct StageArgs {
   const double4 *met1d;       // per padded index: {tan, cos^2/R^2, sin cos/R, R sec^2}
   const double *phibar;       // mean depth per member
   float4 *bnd32;              // raw boundary copy of the increment
+  double *prec;  // TMA form: linear references of the step's first stage per (member, panel, tile), 12 words each
   double two_omega;
   float wd, wt;  // increment = wd * (input increment) + wt * tendency (RK3/RK4 weights)
 };
@@ -405,8 +406,9 @@ struct Tile {
   static constexpr int TOTAL = YR + 3 * I;
   // split precision, after the R arrays: 1-D metric tables [LX] and [LY] double4,
   // then two buffers (alternate work items of the TMA form) of the per-tile
-  // linear references of E, u, v: planes [3][3] double, reference-point values
-  // [3][3] double, slopes [2][3] float
+  // linear references of E, u, v: planes [3][3] double and slopes [2][3] float
+  // (together the 96-byte record a first stage stores and later stages load),
+  // then reference-point values [3][3] double
   static constexpr size_t MET_OFF = ((size_t)TOTAL * sizeof(R) + 31) / 32 * 32;
   static constexpr size_t PLANE_OFF = MET_OFF + (size_t)(LX + LY) * sizeof(double4);
   static constexpr size_t PLANE_BYTES = 176;  // 18 doubles + 6 floats, a 16-byte multiple
@@ -522,8 +524,8 @@ __global__ void __launch_bounds__(NT, MINB)
   double4 *metx = reinterpret_cast<double4 *>(smraw + T::MET_OFF);  // split precision: [LX] then [LY]
   const double4 *mety = metx + LX;
   double *plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF);  // [3] {value at (H, H), d/dlx, d/dly}
-  double *qref = plane + 9;                                            // [3 points][3]
-  float *slope = reinterpret_cast<float *>(qref + 9);                  // [x, y][3]: derivative per radian
+  float *slope = reinterpret_cast<float *>(plane + 9);                 // [x, y][3]: derivative per radian
+  double *qref = plane + 12;                                           // [3 points][3]
   int pb = 0;  // TMA form: plane buffer of the current work item
   uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + T::bar_off(MIXED));
   const int ntile = g.tiles_x * g.tiles_y;
@@ -559,6 +561,7 @@ __global__ void __launch_bounds__(NT, MINB)
       nx = min(LX, g.np - X0);
       ny = min(T::LY, g.np - Y0);
       bytes += (uint32_t)(nx + ny) * sizeof(double4);
+      if constexpr (!first_stage(KIND)) bytes += 96;  // the item's linear references
     }
     mbar_arrive_expect_tx(bar, bytes);
     const int srow = (mem * 6 + panel) * g.np + Y0;  // row of a per-member field
@@ -569,6 +572,11 @@ __global__ void __launch_bounds__(NT, MINB)
     if constexpr (MIXED) {
       bulk_load(metx, a.met1d + X0, (uint32_t)nx * sizeof(double4), bar);
       bulk_load(metx + LX, a.met1d + Y0, (uint32_t)ny * sizeof(double4), bar);
+      // later stages of a step take the linear references the step's first
+      // stage fitted for this tile, into the buffer the item will use
+      if constexpr (!first_stage(KIND))
+        bulk_load(smraw + T::PLANE_OFF + pb * T::PLANE_BYTES,
+                  a.prec + ((long long)(mem * 6 + panel) * ntile + it.ty * g.tiles_x + it.tx) * 12, 96u, bar);
     }
   };
   // 1 / (full tile width in radians), x and y (split precision's linear references)
@@ -589,8 +597,8 @@ __global__ void __launch_bounds__(NT, MINB)
     // alternate buffers: warp 0 fits the next item's references while the
     // other warps may still read this item's slopes in phase A
     plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF + pb * T::PLANE_BYTES);
-    qref = plane + 9;
-    slope = reinterpret_cast<float *>(qref + 9);
+    slope = reinterpret_cast<float *>(plane + 9);
+    qref = plane + 12;
     pb ^= 1;
   }
   int tx, ty, panel, mem;
@@ -796,7 +804,19 @@ __global__ void __launch_bounds__(NT, MINB)
       bool got = true;
       if (threadIdx.x < 32) {
         got = __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity));
-        if (got) fit_planes_warp0();
+        if constexpr (first_stage(KIND)) {
+          // the step's first stage fits the item's references and stores them
+          // for the later stages (whose copies bring them in with the tile)
+          if (got) {
+            fit_planes_warp0();
+            __syncwarp();
+            if (threadIdx.x < 12) {
+              double w;  // one 8-byte word of the record (planes, then the packed slopes)
+              memcpy(&w, reinterpret_cast<const char *>(plane) + 8 * threadIdx.x, 8);
+              a.prec[((long long)(mem * 6 + panel) * ntile + ty * g.tiles_x + tx) * 12 + threadIdx.x] = w;
+            }
+          }
+        }
       }
       bad = __syncthreads_or(!got);
     } else {
