@@ -511,8 +511,11 @@ __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddep
 // TMA: persistent form -- each CTA walks work items (tile, panel, member)
 // blockIdx.x, blockIdx.x + gridDim.x, ...; the next item's input fields are
 // copied into a shared-memory staging area by TMA while the current item's
-// sweeps and update run.  Otherwise one CTA per (tile, panel, member) loads
-// its fields with ordinary loads.
+// sweeps and update run.  A work item has three block barriers (after the
+// copy wait, after phase 0, after the sweeps); split precision fits the
+// linear references in the step's first stage and stores them, and the later
+// stages' copies bring them in with the tile.  Otherwise one CTA per (tile,
+// panel, member) loads its fields with ordinary loads.
 template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA>
 __global__ void __launch_bounds__(NT, MINB)
     stage_kernel(const GridDesc g, const StageArgs a, const __grid_constant__ TileMaps tm) {
@@ -594,8 +597,9 @@ __global__ void __launch_bounds__(NT, MINB)
   const int wfirst = TMA ? (int)blockIdx.x : 0, wstep = TMA ? (int)gridDim.x : 1, wend = TMA ? tm.total : 1;
   for (int wi = wfirst; wi < wend; wi += wstep) {
   if constexpr (TMA && MIXED) {
-    // alternate buffers: warp 0 fits the next item's references while the
-    // other warps may still read this item's slopes in phase A
+    // alternate buffers: the next item's references (fitted by warp 0, or
+    // copied in with the tile) land while other warps may still read this
+    // item's slopes in phase A
     plane = reinterpret_cast<double *>(smraw + T::PLANE_OFF + pb * T::PLANE_BYTES);
     slope = reinterpret_cast<float *>(plane + 9);
     qref = plane + 12;
