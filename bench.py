@@ -299,16 +299,17 @@ def serving_block(count):
     """The serving stream's first `count` requests through the continuous-batching
     server (split precision) and through the plain FP64 one-request-at-a-time loop."""
     from mcv_sw_b200 import serving
-    reqs, geoms = serving.make_requests(count)
+    reqs, geoms = serving.make_requests(count, specs=True)
     keys = sorted({r.key for r in reqs})
-    srv = serving.ForecastServer(precision="mixed", geoms=geoms)
+    srv = serving.ForecastServer(precision="mixed", geoms=geoms, device_setup=True)
     srv.prepare(keys)
     res = srv.run(reqs)
     stats = dict(srv.stats)
     srv.close()
-    base = serving.run_one_at_a_time(reqs, precision="fp64", geoms=geoms)
+    base = serving.run_one_at_a_time(reqs, precision="fp64", geoms=geoms, device_setup=True)
     return {"requests": count, "stream": "Poisson 20 req/s (seed 4), MCV3/MCV4 50/50, Nc 48/96/192/384 "
-                                         "(.4/.3/.2/.1), 6-120 h, half with mountains; RK3_TVD, CFL 0.45",
+                                         "(.4/.3/.2/.1), 6-120 h, half with mountains; RK3_TVD, CFL 0.45; "
+                                         "geometry and initial states generated on the device at admission",
             "server_mixed": serving.summarize(res), "server_stats": stats,
             "one_at_a_time_fp64": serving.summarize(base)}
 

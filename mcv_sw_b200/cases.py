@@ -209,6 +209,20 @@ def serving_dt(geom, cfl=0.45):
     return cfl_dt(geom, u, v, phi, cfl)
 
 
+def serving_spec(radius, req):
+    """The seeded balanced-flow spec of a serving request (the draws of
+    serving_state), for initial states generated on the device."""
+    return balanced_flow_spec(_Radius(radius), np.random.default_rng(req["seed"]), 38.6, 0.05, 8, 10.0,
+                              mountain=req["mountain"])
+
+
+class _Radius:
+    """Stands in for a geometry where only the radius is read."""
+
+    def __init__(self, radius):
+        self.radius = float(radius)
+
+
 def serving_state(geom, req, scheme="RK3_TVD"):
     rng = np.random.default_rng(req["seed"])
     zw, mw, phi, phis, meta = balanced_flow(geom, rng, 38.6, 0.05, 8, 10.0, mountain=req["mountain"])

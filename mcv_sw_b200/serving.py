@@ -14,6 +14,11 @@ and their slots freed for the next requests.  A request's result does not
 depend on what else runs: each member's arithmetic reads only that member's
 data, whatever slot, pool or launch it shares.
 
+With device_setup the pools build their geometry on the device
+(mcv_set_geometry_equiangular) and a request that carries a seeded spec
+instead of host arrays is admitted by generating its initial state on the
+device (mcv_set_member_balanced_flow): nothing of the state crosses PCIe.
+
 The reference runs one forecast per process (src/MCV_SW.F90); it has no
 serving layer.  `run_one_at_a_time` is the plain loop the server is compared
 with: one request after the other, each on its own single-member handle.
@@ -35,10 +40,11 @@ class Request:
     order: int
     nc: int
     hours: float  # forecast length; rounded up to whole steps of the group's dt
-    phi_s: np.ndarray
-    u: np.ndarray
-    v: np.ndarray
-    phi: np.ndarray
+    phi_s: np.ndarray = None  # initial state as host arrays, or ...
+    u: np.ndarray = None
+    v: np.ndarray = None
+    phi: np.ndarray = None
+    spec: dict = None  # ... a seeded balanced-flow spec generated on the device
 
     @property
     def key(self):
@@ -67,13 +73,17 @@ class Result:
         return self.nsteps * self.dt / 86400.0
 
 
-def make_requests(count, seed=4, rate=20.0, radius=cases.EARTH_RADIUS, geoms=None):
+def make_requests(count, seed=4, rate=20.0, radius=cases.EARTH_RADIUS, geoms=None, specs=False):
     """The seeded serving stream: Poisson arrivals, MCV3/MCV4 with probability
     0.5, Nc from {48, 96, 192, 384} (0.4/0.3/0.2/0.1), 6-120 h, balanced tilted
-    zonal flow + seeded harmonics, half with a seeded mountain."""
+    zonal flow + seeded harmonics, half with a seeded mountain.  specs=True:
+    requests carry the seeded spec instead of host arrays (device admission)."""
     geoms = {} if geoms is None else geoms
     out = []
     for r in cases.serving_requests(seed=seed, rate=rate, count=count):
+        if specs:
+            out.append(Request(r["id"], r["t"], r["order"], r["nc"], r["hours"], spec=cases.serving_spec(radius, r)))
+            continue
         key = (r["order"], r["nc"])
         if key not in geoms:
             geoms[key] = api.Geometry(r["order"], r["nc"], radius)
@@ -91,7 +101,10 @@ class _Pool:
         self.bytes = server.footprint(key, slots)
         self.stepper = server.stepper_factory(key[0], key[1], self.dt, server.scheme, members=slots,
                                               precision=server.precision, radius=server.radius)
-        self.stepper.set_geometry(server.geometry(key))
+        if server.device_setup:
+            self.stepper.set_geometry_equiangular()
+        else:
+            self.stepper.set_geometry(server.geometry(key))
         self.req = [None] * slots  # request held by each slot
         self.left = [0] * slots  # steps still to take
         self.admitted = [0.0] * slots
@@ -121,12 +134,16 @@ class ForecastServer:
     chunk_ms: target GPU time of one chunk, which bounds how long an arriving
     request waits for a busy pool.  tile: stage-kernel tile index used by every
     pool (None: each pool's autotuner chooses); split-precision results are
-    reproducible bit for bit only on the same tile shape."""
+    reproducible bit for bit only on the same tile shape.  device_setup: pools
+    build their geometry on the device, and requests carrying a spec get their
+    initial state generated there."""
 
     def __init__(self, precision="mixed", scheme="RK3_TVD", hbm_budget=None, slot_bytes=8e9, max_slots=32,
                  chunk_ms=25.0, tile=None, radius=cases.EARTH_RADIUS, keep_states=False, poll_s=2e-4,
-                 geoms=None, stepper_factory=None, footprint_fn=None, memory_fn=None, clock=time.perf_counter):
+                 geoms=None, stepper_factory=None, footprint_fn=None, memory_fn=None, clock=time.perf_counter,
+                 device_setup=False):
         self.precision, self.scheme, self.radius = precision, scheme, radius
+        self.device_setup = device_setup
         self.slot_bytes, self.max_slots, self.chunk_ms = slot_bytes, max_slots, chunk_ms
         self.tile, self.keep_states, self.poll_s, self.clock = tile, keep_states, poll_s, clock
         self.stepper_factory = stepper_factory or api.Stepper
@@ -195,10 +212,7 @@ class ForecastServer:
             pool = self._new_pool(key)
             if pool is None:
                 continue
-            g = self.geometry(key)
-            zw, mw, phi, phis, _ = cases.balanced_flow(g, np.random.default_rng(0), lmax=0)
-            u, v = api.sphere_to_cov(g, zw, mw)
-            pool.stepper.set_member(0, phis, u, v, phi)
+            _stand_in(pool.stepper, self, key)
             pool.stepper.set_active([0])
             pool.stepper.step(1)
             pool.stepper.set_active([])
@@ -225,7 +239,7 @@ class ForecastServer:
         return self._place(p, 0, req, now)
 
     def _place(self, pool, s, req, now):
-        pool.stepper.set_member(s, req.phi_s, req.u, req.v, req.phi)
+        _load(pool.stepper, s, req)
         pool.req[s] = req
         pool.left[s] = self.nsteps(req)
         pool.admitted[s] = now
@@ -306,23 +320,45 @@ class ForecastServer:
         return [results[r.id] for r in requests]
 
 
+def _load(stepper, slot, req):
+    """A request's initial state into a member slot: its host arrays, or its
+    spec generated on the device."""
+    if req.spec is not None:
+        stepper.set_member_balanced_flow(slot, req.spec)
+    else:
+        stepper.set_member(slot, req.phi_s, req.u, req.v, req.phi)
+
+
+def _stand_in(stepper, server, key):
+    """A plain balanced flow in member 0 (warm-up before a stream)."""
+    if server.device_setup:
+        stepper.set_member_balanced_flow(0, cases.balanced_flow_spec(cases._Radius(server.radius),
+                                                                     np.random.default_rng(0), lmax=0))
+        return
+    g = server.geometry(key)
+    zw, mw, phi, phis, _ = cases.balanced_flow(g, np.random.default_rng(0), lmax=0)
+    u, v = api.sphere_to_cov(g, zw, mw)
+    stepper.set_member(0, phis, u, v, phi)
+
+
 def run_one_at_a_time(requests, precision="fp64", scheme="RK3_TVD", radius=cases.EARTH_RADIUS, geoms=None,
-                      keep_states=False, tile=None, clock=time.perf_counter):
+                      keep_states=False, tile=None, clock=time.perf_counter, device_setup=False):
     """The plain loop: requests in arrival order, one at a time, each on a
     single-member handle of its grid (handles are created and tuned before the
     stream starts, as the server's are; `tile` pins the stage-kernel shape)."""
-    srv = ForecastServer(precision=precision, scheme=scheme, hbm_budget=1 << 62, radius=radius, geoms=geoms)
+    srv = ForecastServer(precision=precision, scheme=scheme, hbm_budget=1 << 62, radius=radius, geoms=geoms,
+                         device_setup=device_setup)
     steppers = {}
     for r in requests:
         if r.key not in steppers:
-            g = srv.geometry(r.key)
             s = api.Stepper(r.order, r.nc, srv.group_dt(r.key), scheme, members=1, precision=precision, radius=radius)
-            s.set_geometry(g)
+            if device_setup:
+                s.set_geometry_equiangular()
+            else:
+                s.set_geometry(srv.geometry(r.key))
             if tile is not None:
                 s.select_tile(tile)
-            zw, mw, phi, phis, _ = cases.balanced_flow(g, np.random.default_rng(0), lmax=0)
-            u, v = api.sphere_to_cov(g, zw, mw)
-            s.set_member(0, phis, u, v, phi)
+            _stand_in(s, srv, r.key)
             s.step(1)
             steppers[r.key] = s
     out = {}
@@ -334,7 +370,7 @@ def run_one_at_a_time(requests, precision="fp64", scheme="RK3_TVD", radius=cases
         s = steppers[r.key]
         admitted = clock() - t0
         n = srv.nsteps(r)
-        s.set_member(0, r.phi_s, r.u, r.v, r.phi)
+        _load(s, 0, r)
         s.step(n)
         flags = s.check_finite()
         state = s.get_state(0)

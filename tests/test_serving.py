@@ -27,6 +27,14 @@ class FakeStepper:
     def select_tile(self, i):
         pass
 
+    def set_geometry_equiangular(self):
+        self.device_geometry = True
+
+    def set_member_balanced_flow(self, m, spec):
+        assert not self.busy, "member upload while a chunk is in flight"
+        self.seed[m] = spec["marker"]
+        self.steps[m] = 0
+
     def set_member(self, m, phi_s, u, v, phi):
         assert not self.busy, "member upload while a chunk is in flight"
         self.seed[m] = phi.flat[0]
@@ -155,3 +163,16 @@ def test_serving_dt_is_below_the_cfl_limit(order, nc):
     for seed in range(3):
         st = cases.serving_state(g, dict(seed=seed, mountain=bool(seed % 2), hours=6.0))
         assert dt <= cases.cfl_dt(g, st.u, st.v, st.phi, 0.5)
+
+
+def test_device_setup_admits_spec_requests():
+    """device_setup: pools take their geometry on the device and requests that
+    carry a spec are loaded by generating their state there."""
+    specs = [(0.0, 3, 8, 2.0), (0.0, 3, 8, 3.0), (0.001, 4, 8, 1.0), (0.002, 3, 8, 4.0)]
+    reqs = [serving.Request(i, t, o, nc, h, spec={"marker": 100.0 + i}) for i, (t, o, nc, h) in enumerate(specs)]
+    srv = server(device_setup=True)
+    res = srv.run(reqs)
+    for q, r in zip(reqs, res):
+        assert r.state["seed"] == q.spec["marker"]
+        assert r.state["steps"] == r.nsteps == srv.nsteps(q)
+    assert all(getattr(st, "device_geometry", False) for st in FakeStepper.created)

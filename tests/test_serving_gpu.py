@@ -104,3 +104,36 @@ def test_inactive_members_keep_their_state():
             s.step(1)  # nothing to advance
             assert not s.check_finite().any()
             assert s.query()
+
+
+def test_device_admission_stream():
+    """Requests carrying seeded specs, admitted by generating their states on
+    the device into pools whose geometry was built there: each result is the
+    same alone and in the mix (split precision), and an FP64 forecast from a
+    device-built state matches the same forecast from host arrays to the
+    parity bar."""
+    reqs, geoms = serving.make_requests(5, seed=11, rate=200.0, specs=True)
+    for r in reqs:  # short forecasts on small grids keep the test quick
+        r.nc, r.hours = (8 if r.order == 4 else 12), 1.0 + (r.id % 3)
+    srv = serving.ForecastServer(precision="mixed", tile=0, keep_states=True, hbm_budget=4 << 30,
+                                 slot_bytes=64 << 20, chunk_ms=0.5, device_setup=True)
+    mix = srv.run(reqs)
+    srv.close()
+    assert all(r.finite for r in mix)
+    for req, r in zip(reqs, mix):
+        alone = serving.ForecastServer(precision="mixed", tile=0, keep_states=True, hbm_budget=4 << 30,
+                                       slot_bytes=64 << 20, device_setup=True)
+        (a,) = alone.run([serving.Request(req.id, 0.0, req.order, req.nc, req.hours, spec=req.spec)])
+        alone.close()
+        assert same(a, r), req.id
+    req = reqs[0]
+    dev = serving.run_one_at_a_time([req], precision="fp64", keep_states=True, device_setup=True)[0]
+    geom = api.Geometry(req.order, req.nc, cases.EARTH_RADIUS)
+    zw, mw, phi, phis = cases.balanced_flow_from_spec(geom, req.spec)
+    u, v = api.sphere_to_cov(geom, zw, mw)
+    host_req = serving.Request(req.id, 0.0, req.order, req.nc, req.hours, phis, u, v, phi)
+    host = serving.run_one_at_a_time([host_req], precision="fp64", keep_states=True)[0]
+    H, n = geom.H, geom.n
+    for k in ("u", "v", "phi"):
+        a, b = dev.state[k][:, H:H + n, H:H + n], host.state[k][:, H:H + n, H:H + n]
+        assert np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)) <= 1e-12, k
