@@ -80,9 +80,10 @@ int mcv_set_geometry(mcv_handle *h, const double *sqrtG, const double *matrixG, 
  * differ from the host's by a few ulp. */
 int mcv_set_geometry_equiangular(mcv_handle *h);
 
-/* Copy the handle's metric back: sqrtG, G^11, G^12, G^22, f over the padded
- * range (Fortran layout) and the ghost weights iref, coef as (nPVx, nPVHalo);
- * any output may be NULL. */
+/* Copy the handle's metric back (no reference counterpart; it lets a caller
+ * check the geometry a handle holds, e.g. one built on the device): sqrtG,
+ * G^11, G^12, G^22, f over the padded range (Fortran layout) and the ghost
+ * weights iref, coef as (nPVx, nPVHalo); any output may be NULL. */
 int mcv_get_geometry(mcv_handle *h, double *sqrtG, double *ig11, double *ig12, double *ig22, double *f,
                      int *ghost_iref, double *ghost_coef);
 

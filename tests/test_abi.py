@@ -40,6 +40,14 @@ def test_argument_errors_are_reported():
     rc = L.mcv_create(5, 32, 3, 0, 100.0, 6.371e6, 1, ctypes.byref(h))
     assert rc == -1 and b"order" in L.mcv_last_error()
     assert L.mcv_footprint_bytes(4, 256, 3, 0, 1) > 0
+    # checked before any device call
+    for limit in (0.0, -1.0, 5000.0):
+        with pytest.raises(api.MCVError) as e:
+            api.selftest_wait(False, limit)
+        assert e.value.code == -1
+    assert L.mcv_set_geometry_equiangular(None) == -1
+    assert L.mcv_set_member_balanced_flow(None, 0, 0., 0., 0., 0, None, 0., 0., 0., 0., 1.) == -1
+    assert L.mcv_get_geometry(None, None, None, None, None, None, None, None) == -1
 
 
 @pytest.mark.skipif(os.path.exists("/dev/nvidia0"), reason="checks the no-GPU behaviour")
