@@ -14,7 +14,8 @@ const StageLauncher *stage_launchers_d4_f64(int *count) {
     StageConfig<4, 6, 6, 256, 3, false, 3>::make(),
     StageConfig<4, 8, 8, 320, 2, false, 2>::make(),
     StageConfig<4, 6, 6, 256, 2, false, 0, true>::make(),
-    StageConfig<4, 8, 8, 320, 1, false, 0, true>::make()};
+    StageConfig<4, 8, 8, 320, 1, false, 0, true>::make(),
+    StageConfig<4, 8, 8, 640, 1, false, 2, true>::make()};
   *count = (int)(sizeof(table) / sizeof(table[0]));
   return table;
 }
