@@ -84,8 +84,8 @@ def test_mixed_tile_shapes_agree():
             assert d < TILE_TOL, (i, k, d)
 
 
-@pytest.mark.parametrize("order", [3, 4])
-def test_every_shape_members_and_active_set(order):
+@pytest.mark.parametrize("order,scheme", [(3, "RK3_TVD"), (4, "RK3_TVD"), (4, "RK4")])
+def test_every_shape_members_and_active_set(order, scheme):
     """Each candidate shape (the persistent TMA form included) with three
     members of which two are active: every active member equals a one-member
     run of the same shape bit for bit (a member's arithmetic reads only its own
@@ -93,10 +93,10 @@ def test_every_shape_members_and_active_set(order):
     its state.  Nc = 20 leaves ragged tiles for every shape."""
     geom = api.Geometry(order, 20, cases.EARTH_RADIUS)
     states = [cases.finish(geom, *cases.balanced_flow(geom, np.random.default_rng(40 + m), mountain=bool(m % 2))[:4],
-                           "RK3_TVD", nsteps=2) for m in range(3)]
+                           scheme, nsteps=2) for m in range(3)]
     dt = min(st.dt for st in states)
-    with api.Stepper(order, 20, dt, "RK3_TVD", members=3, precision="mixed", radius=cases.EARTH_RADIUS) as s, \
-            api.Stepper(order, 20, dt, "RK3_TVD", members=1, precision="mixed", radius=cases.EARTH_RADIUS) as one:
+    with api.Stepper(order, 20, dt, scheme, members=3, precision="mixed", radius=cases.EARTH_RADIUS) as s, \
+            api.Stepper(order, 20, dt, scheme, members=1, precision="mixed", radius=cases.EARTH_RADIUS) as one:
         s.set_geometry(geom)
         one.set_geometry(geom)
         for m, st in enumerate(states):
