@@ -311,6 +311,7 @@ StageArgs stage_args(mcv_handle *h, int s, int c) {
   a.fU = h->facc[0]; a.fV = h->facc[1]; a.fP = h->facc[2];
   a.phis32 = h->phis32; a.met1d = h->met1d; a.phibar = h->phibar; a.bnd32 = h->bnd32; a.prec = h->prec;
   a.two_omega = 2. * kOmega;
+  a.r2 = h->radius * h->radius;
   float *const *din = nullptr, *const *dout = nullptr;
   float wd = 0.f, wt = 0.f;
   switch (kind) {

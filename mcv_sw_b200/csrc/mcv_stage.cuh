@@ -77,6 +77,7 @@ struct StageArgs {
   float4 *bnd32;              // raw boundary copy of the increment
   double *prec;  // TMA form: linear references of the step's first stage per (member, panel, tile), 12 words each
   double two_omega;
+  double r2;  // radius squared (split precision: 1/sqrtG from the 1-D tables)
   float wd, wt;  // increment = wd * (input increment) + wt * tendency (RK3/RK4 weights)
 };
 
@@ -331,8 +332,10 @@ __device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, con
     cq[m] = q[m * S];
   }
   float2 fR = polyfit_right2<D>(cf, ip), qR = polyfit_right2<D>(cq, ip);
+  cf[0] = cf[D - 1];  // the point the halo cell and the first cell share
+  cq[0] = cq[D - 1];
 #pragma unroll
-  for (int m = 0; m < D; ++m) {
+  for (int m = 1; m < D; ++m) {
     cf[m] = f[(D - 1 + m) * S];
     cq[m] = q[(D - 1 + m) * S];
   }
@@ -343,8 +346,10 @@ __device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, con
   for (int c = 0; c < NMAX; ++c) {
     if (c < ncells) {
       float2 nf[D], nq[D];
+      nf[0] = cf[D - 1];
+      nq[0] = cq[D - 1];
 #pragma unroll
-      for (int m = 0; m < D; ++m) {
+      for (int m = 1; m < D; ++m) {
         nf[m] = f[((c + 2) * (D - 1) + m) * S];
         nq[m] = q[((c + 2) * (D - 1) + m) * S];
       }
@@ -393,7 +398,8 @@ struct Tile {
   static constexpr bool PAIRED = std::is_same<R, float>::value;
   static constexpr int U = 0, V = A, E = 2 * A, PG = 3 * A, PGU = 4 * A, PGV = 5 * A;
   static constexpr int XF = 2 * A, XQ = 4 * A, YF = 6 * A, YQ = 8 * A;  // in floats (even: float2-aligned)
-  // ... interior-only arrays ...
+  // ... interior-only arrays: sqrtG, cU, cV (split precision: 1/sqrtG, cU,
+  // cV, sqrtG f) ...
   static constexpr int SG = (PAIRED ? 10 : 6) * A, CU = SG + I, CV = CU + I, FC = CV + I;
   // ... interface eigenvalues and upwind signs ...
   static constexpr int LAMX = FC + I;                // [TY][CX+1]
@@ -437,15 +443,17 @@ struct Tile {
 // u, v, phiG, phiG cU, phiG cV} are the fields the sweeps difference.
 struct MixPoint {
   double q[6];
-  double sg, cu, cv, g11, g22, fc;
+  double sg, cu, cv, g11, g22, fc, rsg;
 };
 __device__ __forceinline__ void mix_point(MixPoint &o, const double4 mx, const double4 my, double u, double v,
-                                          double p, double phs, double phibar, int panel, double two_omega) {
+                                          double p, double phs, double phibar, int panel, double two_omega,
+                                          double r2) {
   // equiangular metric from the separable 1-D tables {tan, cos^2/R^2, sin cos/R,
   // R/cos^2} (projection_mod.F90:150-211 with cos^2 y (1 + tan^2 y) = 1)
   const double rho2 = 1. + mx.x * mx.x + my.x * my.x;
   const double rinv = rsqrt(rho2);
   o.sg = mx.w * my.w * (rinv * rinv * rinv);
+  o.rsg = (rho2 * rho2 * rinv) * ((mx.y * my.y) * r2);  // 1/sqrtG: 1/(R sec^2) = R cos^2/R^2
   o.g11 = rho2 * mx.y;
   o.g22 = rho2 * my.y;
   const double g12 = rho2 * (mx.z * my.z);
@@ -674,7 +682,7 @@ __global__ void __launch_bounds__(NT, MINB)
         p += (double)__ldg(t_dp + o);
       }
       MixPoint mp;
-      mix_point(mp, a.met1d[X0 + lx], a.met1d[Y0 + ly], u, v, p, phs, phibar, panel, a.two_omega);
+      mix_point(mp, a.met1d[X0 + lx], a.met1d[Y0 + ly], u, v, p, phs, phibar, panel, a.two_omega, a.r2);
 #pragma unroll
       for (int q = 0; q < 3; ++q) qref[threadIdx.x * 3 + q] = mp.q[q];
     }
@@ -712,7 +720,7 @@ __global__ void __launch_bounds__(NT, MINB)
         p += (double)stg32(6, lx, ly);
       }
       MixPoint mp;
-      mix_point(mp, metx[lx], mety[ly], u, v, p, phs, phibar, panel, a.two_omega);
+      mix_point(mp, metx[lx], mety[ly], u, v, p, phs, phibar, panel, a.two_omega, a.r2);
 #pragma unroll
       for (int j = 0; j < 3; ++j) q[j] = mp.q[j];
     }
@@ -739,7 +747,9 @@ __global__ void __launch_bounds__(NT, MINB)
 
   // one loaded point: r = {u, v, phi, phi_s, sqrtG, G^11, G^12, G^22} (FP64
   // policy) or {Y_u, Y_v, Y_phi} with f = {phi_s, d_u, d_v, d_phi} (split)
-  auto point = [&](int idx, int lx, int ly, const double *r, const float *f, const double4 &mx, const double4 &my) {
+  // (X, Y) = (lx - H, ly - H) as doubles, the linear references' coordinates
+  auto point = [&](int idx, int lx, int ly, double X, double Y, const double *r, const float *f, const double4 &mx,
+                   const double4 &my) {
     // interior points also keep sqrtG, cU, cV (and f) and form the interface
     // eigenvalues and upwind signs; split precision rounds those to FP32 here
     auto interior = [&](R sg, R cu, R cv, R fc, R g11, R g22, R phi) {
@@ -781,21 +791,21 @@ __global__ void __launch_bounds__(NT, MINB)
         p64 += (double)f[3];
       }
       MixPoint mp;
-      mix_point(mp, mx, my, u64, v64, p64, (double)f[0], phibar, panel, a.two_omega);
-      const double X = (double)(lx - H), Y = (double)(ly - H);
+      mix_point(mp, mx, my, u64, v64, p64, (double)f[0], phibar, panel, a.two_omega, a.r2);
       const float e = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
       const float uu = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
       const float vv = (float)(mp.q[2] - (plane[6] + plane[7] * X + plane[8] * Y));
-      const float pg = (float)mp.q[3];
+      // the mass fluxes as FP32 products of the rounded phiG and winds
+      const float pg = (float)mp.q[3], cu = (float)mp.cu, cv = (float)mp.cv;
       float2 *s2 = reinterpret_cast<float2 *>(sm);
       sm[T::U + idx] = uu;
       sm[T::V + idx] = vv;
-      s2[T::XF / 2 + idx] = make_float2(e, (float)mp.q[4]);
+      s2[T::XF / 2 + idx] = make_float2(e, pg * cu);
       s2[T::XQ / 2 + idx] = make_float2(uu, pg);
-      s2[T::YF / 2 + idx] = make_float2(e, (float)mp.q[5]);
+      s2[T::YF / 2 + idx] = make_float2(e, pg * cv);
       s2[T::YQ / 2 + idx] = make_float2(vv, pg);
-      if (inner)
-        interior((float)mp.sg, (float)mp.cu, (float)mp.cv, (float)mp.fc, (float)mp.g11, (float)mp.g22, (float)p64);
+      // split precision keeps 1/sqrtG and sqrtG f for the assembly
+      if (inner) interior((float)mp.rsg, cu, cv, (float)(mp.sg * mp.fc), (float)mp.g11, (float)mp.g22, (float)p64);
     }
   };
 
@@ -856,13 +866,15 @@ __global__ void __launch_bounds__(NT, MINB)
       if (lx < lxe) {
         const bool xh = (lx < H) || (lx >= lxe - H);
         const double4 mx = MIXED ? metx[lx] : double4{};
-        for (int ly = threadIdx.x >> 5; ly < lye; ly += NT / 32) {
+        const double X = (double)(lx - H);
+        double Y = (double)((int)(threadIdx.x >> 5) - H);
+        for (int ly = threadIdx.x >> 5; ly < lye; ly += NT / 32, Y += (double)(NT / 32)) {
           const bool yh = (ly < H) || (ly >= lye - H);
           if (xh && yh) continue;  // tile corners are never read
           double r[8];
           float f[4];
           staged(lx, ly, r, f);
-          point(ly * LX + lx, lx, ly, r, f, mx, MIXED ? mety[ly] : mx);
+          point(ly * LX + lx, lx, ly, X, Y, r, f, mx, MIXED ? mety[ly] : mx);
         }
       }
     } else {
@@ -874,7 +886,7 @@ __global__ void __launch_bounds__(NT, MINB)
         float f[4];
         staged(lx, ly, r, f);
         const double4 zero{};
-        point(idx, lx, ly, r, f, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
+        point(idx, lx, ly, (double)(lx - H), (double)(ly - H), r, f, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
       }
     }
   } else {
@@ -936,7 +948,8 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
         for (int j = 0; j < 4; ++j) ff[j] = f[j][k];
         const double4 zero{};
-        point(idx, lx, ly, rr, ff, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
+        point(idx, lx, ly, (double)(lx - H), (double)(ly - H), rr, ff, MIXED ? metx[lx] : zero,
+              MIXED ? mety[ly] : zero);
       }
     }
   }
@@ -1197,9 +1210,10 @@ __global__ void __launch_bounds__(NT, MINB)
     const int it = base0 + threadIdx.x + k * NT;
     const int r = it / T::TX, q = it - r * T::TX;
     const long long go = mbase + tbase + ((H + r) * g.P + (H + q));
+    // FP64 policy: SG = sqrtG; split precision: SG = 1/sqrtG, FC = sqrtG f
     const R sg = sm[T::SG + it], cu = sm[T::CU + it], cv = sm[T::CV + it];
     const R fc = MIXED ? sm[T::FC + it] : (R)gf[k];
-    const R rsg = R(1) / sg;
+    const R rsg = MIXED ? sg : R(1) / sg;
     R flux_x = sm[T::XR + it], dvdx = sm[T::XR + 2 * T::I + it];
     R flux_y = sm[T::YR + it], dudy = sm[T::YR + 2 * T::I + it];
     const R div_x = sm[T::XR + T::I + it], div_y = sm[T::YR + T::I + it];
@@ -1210,10 +1224,18 @@ __global__ void __launch_bounds__(NT, MINB)
       flux_y += slope[3 + 0];
       dudy += slope[3 + 1];
     }
-    const R vort = (dvdx - dudy) * rsg;
     const R tP = -div_x - div_y;
-    const R tU = -flux_x + sg * (vort + fc) * cv;
-    const R tV = -flux_y - sg * (vort + fc) * cu;
+    R tU, tV;
+    if constexpr (MIXED) {
+      // sqrtG (vort + f) = (dvdx - dudy) + sqrtG f
+      const R ab = (dvdx - dudy) + fc;
+      tU = -flux_x + ab * cv;
+      tV = -flux_y - ab * cu;
+    } else {
+      const R vort = (dvdx - dudy) * rsg;
+      tU = -flux_x + sg * (vort + fc) * cv;
+      tV = -flux_y - sg * (vort + fc) * cu;
+    }
     const int sidx = (r + H) * LX + (q + H);
     double uo, vo, po;  // values the boundary copy records
     if constexpr (!MIXED) {
