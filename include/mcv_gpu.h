@@ -219,6 +219,70 @@ long long mcv_footprint_bytes(int order, int nc, int scheme, int precision, int 
 int mcv_device_memory(long long *free_bytes, long long *total_bytes);
 
 /* ---------------------------------------------------------------------
+ * Forecast server: continuous batching of many forecasts on one GPU.
+ * No counterpart in the reference, which runs one forecast per process
+ * (src/MCV_SW.F90).  Requests of any order, Nc, dt and length are queued;
+ * each is admitted, by HBM footprint, into a free member slot of a pool (a
+ * handle of its grid (order, Nc, dt) with device geometry, built by
+ * mcv_set_geometry_equiangular), and advanced with the pool's other members
+ * in chunks of RK steps on the pool's own stream, so pools of different grids
+ * overlap on the GPU.  A request's result is bit for bit the one a plain
+ * handle with the same tile shape gives it alone.  A server is not
+ * thread-safe.
+ * ------------------------------------------------------------------- */
+typedef struct mcv_server mcv_server;
+
+/* precision, scheme, radius: as mcv_create, for every pool.  hbm_budget:
+ * bytes the pools may hold (<= 0: 85% of the device's free memory now).  A
+ * pool gets as many slots as fit in slot_bytes (1..max_slots).  chunk_ms: GPU
+ * time of one chunk, which bounds how long a request waits for a busy pool of
+ * its grid.  tile: stage-kernel candidate of every pool (mcv_select_tile), or
+ * -1 for each pool's autotuner. */
+int mcv_server_create(int precision, int scheme, double radius, long long hbm_budget, long long slot_bytes,
+                      int max_slots, double chunk_ms, int tile, mcv_server **out);
+
+/* Queue a forecast of nsteps RK steps of dt seconds from the host state
+ * (phi_s, u, v, phi over the padded range, as mcv_set_member; copied).
+ * *id identifies it (ids count up from 1).  MCV_ERR_NOMEM if even a
+ * one-slot pool of its grid exceeds the budget. */
+int mcv_server_submit(mcv_server *s, int order, int nc, double dt, long long nsteps, const double *phi_s,
+                      const double *u, const double *v, const double *phi, long long *id);
+
+/* Queue a forecast whose initial state is generated on the device at
+ * admission (the arguments of mcv_set_member_balanced_flow). */
+int mcv_server_submit_balanced_flow(mcv_server *s, int order, int nc, double dt, long long nsteps, double gh0,
+                                    double u0, double alpha, int lmax, const double *coef, double rms,
+                                    double mountain_h0, double lon_c, double lat_c, double efold, long long *id);
+
+/* Create the pool of a grid ahead of its requests and step a resting state
+ * once, so that autotuning and graph capture are not part of a request's
+ * latency.  Blocks. */
+int mcv_server_prepare(mcv_server *s, int order, int nc, double dt);
+
+/* One pass of the request loop; never waits for the GPU.  Retires the chunks
+ * that have ended (checking finished forecasts for NaN/Inf and downloading
+ * them), admits waiting requests that fit, first come first served, and
+ * queues the next chunk of every idle pool.  Writes up to max_ids ids of
+ * forecasts finished since the last poll to ids (*n_ids of them); the rest
+ * are reported by later polls.  A pool's first chunk autotunes its stage
+ * kernel and captures its step graphs, which blocks (see mcv_server_prepare). */
+int mcv_server_poll(mcv_server *s, long long *ids, int max_ids, int *n_ids);
+
+/* Copy out and release a finished forecast: u, v, phi, phiG over the padded
+ * range (any pointer may be NULL), its step count and *finite = 0 if its
+ * state holds a NaN or Inf.  MCV_BUSY if it is still queued or running. */
+int mcv_server_result(mcv_server *s, long long id, double *u, double *v, double *phi, double *phiG,
+                      long long *nsteps, int *finite);
+
+/* stats[9]: waiting requests, running forecasts, finished results not yet
+ * taken, pools, pools with a chunk on the GPU, bytes the pools hold, pools
+ * created, pools evicted, chunks retired. */
+int mcv_server_stats(mcv_server *s, long long *stats);
+
+/* Release every pool and the server (waits for queued work). */
+int mcv_server_destroy(mcv_server *s);
+
+/* ---------------------------------------------------------------------
  * Host-side init chain (the caller's side of the boundary; provided so C,
  * C++ and Python callers without the Fortran setup can build inputs).
  * ------------------------------------------------------------------- */

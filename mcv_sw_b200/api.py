@@ -94,6 +94,22 @@ def lib():
         "mcv_ic_add_rossby_wave": (ctypes.c_int, [ctypes.c_longlong, _D, _D, ctypes.c_double, ctypes.c_int,
                                                   ctypes.c_double, _D, _D, _D]),
         "mcv_sphere_to_cov": (ctypes.c_int, [ctypes.c_longlong, _D, _D, _D, _D, _D, _D]),
+        "mcv_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_longlong,
+                                             ctypes.c_longlong, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                             ctypes.POINTER(vp)]),
+        "mcv_server_submit": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_longlong,
+                                             _D, _D, _D, _D, ctypes.POINTER(ctypes.c_longlong)]),
+        "mcv_server_submit_balanced_flow": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                           ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
+                                                           ctypes.c_double, ctypes.c_int, _D, ctypes.c_double,
+                                                           ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                           ctypes.c_double, ctypes.POINTER(ctypes.c_longlong)]),
+        "mcv_server_prepare": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+        "mcv_server_poll": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, _I]),
+        "mcv_server_result": (ctypes.c_int, [vp, ctypes.c_longlong, _D, _D, _D, _D,
+                                             ctypes.POINTER(ctypes.c_longlong), _I]),
+        "mcv_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
+        "mcv_server_destroy": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -382,3 +398,94 @@ class Stepper:
         ms, en = ctypes.c_double(), ctypes.c_double()
         _check(lib().mcv_mass_energy(self.h, int(m), ctypes.byref(ms), ctypes.byref(en)))
         return ms.value, en.value
+
+
+SERVER_STATS = ("waiting", "running", "unclaimed", "pools", "busy_pools", "pool_bytes", "pools_created",
+                "pools_evicted", "chunks")
+
+
+class Server:
+    """The native forecast server (mcv_server_*): requests are queued with
+    submit / submit_spec, mcv_server_poll runs one pass of the request loop,
+    and a finished forecast's state is taken with result."""
+
+    def __init__(self, precision="mixed", scheme="RK3_TVD", radius=6371220.0, hbm_budget=0, slot_bytes=8 << 30,
+                 max_slots=32, chunk_ms=25.0, tile=-1):
+        self.precision, self.scheme, self.radius = precision, scheme, float(radius)
+        s = ctypes.c_void_p()
+        _check(lib().mcv_server_create(PRECISIONS[precision], SCHEMES[scheme], self.radius, int(hbm_budget),
+                                       int(slot_bytes), int(max_slots), float(chunk_ms), int(tile), ctypes.byref(s)))
+        self.s = s
+        self.grids = {}  # request id -> (order, nc)
+
+    def close(self):
+        if getattr(self, "s", None):
+            lib().mcv_server_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, order, nc, dt, nsteps, phi_s, u, v, phi):
+        npx, _, _ = grid_sizes(order, nc)
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (phi_s, u, v, phi)]
+        if any(a.size != 6 * npx * npx for a in arrs):
+            raise ValueError(f"state arrays must hold 6 x {npx} x {npx} points")
+        rid = ctypes.c_longlong()
+        _check(lib().mcv_server_submit(self.s, int(order), int(nc), float(dt), int(nsteps), *[_dp(x) for x in arrs],
+                                       ctypes.byref(rid)))
+        self.grids[rid.value] = (int(order), int(nc))
+        return rid.value
+
+    def submit_spec(self, order, nc, dt, nsteps, spec):
+        """A forecast whose initial state the device generates from a
+        balanced-flow spec (cases.balanced_flow_spec) at admission."""
+        lmax = int(spec["lmax"])
+        coef = np.ascontiguousarray(spec["coef"], dtype=np.float64) if lmax else None
+        mt = spec.get("mountain")
+        rid = ctypes.c_longlong()
+        _check(lib().mcv_server_submit_balanced_flow(
+            self.s, int(order), int(nc), float(dt), int(nsteps), float(spec["gh0"]), float(spec["u0"]),
+            float(spec["alpha"]), lmax, _dp(coef), float(spec["rms"]), float(mt["h0"]) if mt else 0.0,
+            float(mt["lon"]) if mt else 0.0, float(mt["lat"]) if mt else 0.0, float(mt["efold"]) if mt else 1.0,
+            ctypes.byref(rid)))
+        self.grids[rid.value] = (int(order), int(nc))
+        return rid.value
+
+    def prepare(self, order, nc, dt):
+        _check(lib().mcv_server_prepare(self.s, int(order), int(nc), float(dt)))
+
+    def poll(self, max_ids=64):
+        """One pass of the request loop; ids of the forecasts finished since the last poll."""
+        ids = (ctypes.c_longlong * max(1, max_ids))()
+        n = ctypes.c_int()
+        _check(lib().mcv_server_poll(self.s, ids, int(max_ids), ctypes.byref(n)))
+        return list(ids[: n.value])
+
+    def result(self, rid):
+        """(state dict u, v, phi, phiG over the padded range, steps taken, finite), or None while running."""
+        order, nc = self.grids[rid]
+        npx, _, _ = grid_sizes(order, nc)
+        out = {k: np.empty((6, npx, npx)) for k in ("u", "v", "phi", "phiG")}
+        steps, fin = ctypes.c_longlong(), ctypes.c_int()
+        rc = lib().mcv_server_result(self.s, int(rid), *[_dp(out[k]) for k in ("u", "v", "phi", "phiG")],
+                                     ctypes.byref(steps), ctypes.byref(fin))
+        if rc == BUSY:
+            return None
+        _check(rc)
+        del self.grids[rid]
+        return out, steps.value, bool(fin.value)
+
+    def stats(self):
+        st = (ctypes.c_longlong * 9)()
+        _check(lib().mcv_server_stats(self.s, st))
+        return dict(zip(SERVER_STATS, list(st)))

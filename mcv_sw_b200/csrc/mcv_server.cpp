@@ -1,0 +1,455 @@
+// mcv_server.cpp -- continuous-batching forecast server behind the C ABI
+// (mcv_server_*).  The reference runs one forecast per process
+// (src/MCV_SW.F90); it has no serving layer.  This is the native form of the
+// request loop: requests of different order, Nc and length are queued,
+// admitted by HBM footprint into member slots of device-resident pools, and
+// advanced in chunks of RK steps on the pools' own streams, so pools of
+// different grids run on the GPU at the same time.  It is built only on the
+// handle entry points of mcv_gpu.h (mcv_create, mcv_set_geometry_equiangular,
+// mcv_set_member[_balanced_flow], mcv_set_active, mcv_step_async, mcv_query,
+// mcv_check_finite, mcv_get_state), so a request's arithmetic is exactly that
+// of a plain handle stepped alone on the same tile shape.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <iterator>
+#include <map>
+#include <vector>
+
+#include "../../include/mcv_gpu.h"
+#include "mcv_internal.h"
+
+using mcv::fail;
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+  long long id;
+  int order, nc;
+  double dt;
+  long long nsteps;
+  bool spec;  // initial state generated on the device from the balanced-flow spec
+  std::vector<double> phis, u, v, phi;  // host copies (spec = false)
+  double gh0, u0, alpha, rms, mh0, lon_c, lat_c, efold;
+  int lmax;
+  std::vector<double> coef;
+};
+
+struct Finished {
+  std::vector<double> u, v, phi, phiG;
+  long long nsteps;
+  int finite;
+};
+
+struct Pool {
+  int order, nc;
+  double dt;
+  int slots;
+  long long bytes;
+  mcv_handle *h = nullptr;
+  std::vector<long long> req;   // request id held by each slot, -1: free
+  std::vector<long long> left;  // steps still to take
+  std::vector<long long> total;
+  std::vector<int> active;      // slots the next chunk advances
+  std::vector<int> dev_active;  // slot list the handle was last given
+  bool dev_active_set = false;
+  long long in_flight = 0;  // steps of the chunk on the GPU (0: idle)
+  double launched = 0.;
+  double ms_per_step = -1.;  // measured, or < 0 before the first chunk
+
+  bool same_grid(int o, int n, double d) const { return order == o && nc == n && dt == d; }
+  int free_slot() const {
+    for (int s = 0; s < slots; ++s)
+      if (req[s] < 0) return s;
+    return -1;
+  }
+  bool empty() const {
+    for (long long r : req)
+      if (r >= 0) return false;
+    return true;
+  }
+};
+
+}  // namespace
+
+struct mcv_server {
+  int precision, scheme, tile, max_slots;
+  double radius, chunk_ms;
+  long long budget, slot_bytes;
+  long long next_id = 1;
+  std::deque<Request> waiting;
+  std::vector<Pool *> pools;
+  std::map<long long, Finished> finished;
+  std::deque<long long> unreported;  // finished ids not yet returned by mcv_server_poll
+  long long pools_created = 0, pools_evicted = 0, chunks = 0;
+};
+
+namespace {
+
+long long used_bytes(const mcv_server *s) {
+  long long b = 0;
+  for (const Pool *p : s->pools) b += p->bytes;
+  return b;
+}
+
+long long footprint(const mcv_server *s, int order, int nc, int members) {
+  return mcv_footprint_bytes(order, nc, s->scheme, s->precision, members);
+}
+
+int slots_for(const mcv_server *s, int order, int nc) {
+  const long long per = footprint(s, order, nc, 2) - footprint(s, order, nc, 1);
+  const long long n = s->slot_bytes / std::max(per, 1LL);
+  return (int)std::max(1LL, std::min((long long)s->max_slots, n));
+}
+
+void close_pool(Pool *p) {
+  if (p->h) {
+    mcv_sync(p->h);
+    mcv_destroy(p->h);
+  }
+  delete p;
+}
+
+// A pool of `slots` member slots on the grid (order, nc, dt), or nullptr with
+// *rc = MCV_OK when the budget has no room even after evicting idle empty pools.
+Pool *new_pool(mcv_server *s, int order, int nc, double dt, int *rc) {
+  *rc = MCV_OK;
+  const int slots = slots_for(s, order, nc);
+  const long long need = footprint(s, order, nc, slots);
+  while (used_bytes(s) + need > s->budget) {
+    // evict an idle, empty pool (the largest first)
+    Pool *victim = nullptr;
+    for (Pool *p : s->pools)
+      if (!p->in_flight && p->empty() && (!victim || p->bytes > victim->bytes)) victim = p;
+    if (!victim) return nullptr;
+    s->pools.erase(std::find(s->pools.begin(), s->pools.end(), victim));
+    close_pool(victim);
+    ++s->pools_evicted;
+  }
+  Pool *p = new Pool();
+  p->order = order;
+  p->nc = nc;
+  p->dt = dt;
+  p->slots = slots;
+  p->bytes = need;
+  p->req.assign(slots, -1);
+  p->left.assign(slots, 0);
+  p->total.assign(slots, 0);
+  if ((*rc = mcv_create(order, nc, s->scheme, s->precision, dt, s->radius, slots, &p->h)) != MCV_OK ||
+      (*rc = mcv_set_geometry_equiangular(p->h)) != MCV_OK ||
+      (s->tile >= 0 && (*rc = mcv_select_tile(p->h, s->tile)) != MCV_OK)) {
+    close_pool(p);
+    return nullptr;
+  }
+  s->pools.push_back(p);
+  ++s->pools_created;
+  return p;
+}
+
+int load_member(Pool *p, int slot, const Request &r) {
+  if (r.spec)
+    return mcv_set_member_balanced_flow(p->h, slot, r.gh0, r.u0, r.alpha, r.lmax, r.coef.empty() ? nullptr : r.coef.data(),
+                                        r.rms, r.mh0, r.lon_c, r.lat_c, r.efold);
+  return mcv_set_member(p->h, slot, r.phis.data(), r.u.data(), r.v.data(), r.phi.data());
+}
+
+int place(Pool *p, int slot, const Request &r) {
+  if (int rc = load_member(p, slot, r)) return rc;
+  p->req[slot] = r.id;
+  p->left[slot] = r.nsteps;
+  p->total[slot] = r.nsteps;
+  p->active.push_back(slot);
+  return MCV_OK;
+}
+
+// Admit r if a slot is free now: *placed = 1.  A request waits while the idle
+// pools of its grid are full, a busy pool of its grid has a free slot (it is
+// taken when that pool's chunk ends), or the budget has no room.
+int admit(mcv_server *s, const Request &r, int *placed) {
+  *placed = 0;
+  bool busy_room = false;
+  for (Pool *p : s->pools) {
+    if (!p->same_grid(r.order, r.nc, r.dt)) continue;
+    const int slot = p->free_slot();
+    if (slot < 0) continue;
+    if (p->in_flight) {
+      busy_room = true;
+      continue;
+    }
+    if (int rc = place(p, slot, r)) return rc;
+    *placed = 1;
+    return MCV_OK;
+  }
+  if (busy_room) return MCV_OK;
+  int rc;
+  Pool *p = new_pool(s, r.order, r.nc, r.dt, &rc);
+  if (!p) return rc;
+  if ((rc = place(p, 0, r))) return rc;
+  *placed = 1;
+  return MCV_OK;
+}
+
+long long chunk_steps(const mcv_server *s, const Pool *p) {
+  long long left = p->left[p->active[0]];
+  for (int slot : p->active) left = std::min(left, p->left[slot]);
+  double est = p->ms_per_step;
+  if (est <= 0.) {
+    // before the first chunk: ~1.3e-7 ms per point and step for one member (B200)
+    const double n = 6. * std::pow((double)p->nc * (p->order - 1) + 1., 2.);
+    est = std::max(1.3e-7 * n * (double)p->active.size(), 0.02);
+  }
+  return std::max(1LL, std::min(left, (long long)(s->chunk_ms / est)));
+}
+
+// The pool's chunk has ended: retire the forecasts it completed.
+int finish_chunk(mcv_server *s, Pool *p) {
+  const long long steps = p->in_flight;
+  p->in_flight = 0;
+  ++s->chunks;
+  const double el = (now_ms() - p->launched) / (double)steps;
+  p->ms_per_step = p->ms_per_step < 0. ? el : 0.5 * (p->ms_per_step + el);
+  std::vector<int> done, still;
+  for (int slot : p->active) {
+    p->left[slot] -= steps;
+    (p->left[slot] == 0 ? done : still).push_back(slot);
+  }
+  if (done.empty()) return MCV_OK;
+  std::vector<int> flags(p->slots, 0);
+  const int frc = mcv_check_finite(p->h, flags.data());
+  if (frc != MCV_OK && frc != MCV_ERR_NONFINITE) return frc;
+  int npx, n, halo;
+  mcv_grid_sizes(p->order, p->nc, &npx, &n, &halo);
+  const size_t sz = (size_t)npx * npx * 6;
+  for (int slot : done) {
+    Finished f;
+    f.u.resize(sz);
+    f.v.resize(sz);
+    f.phi.resize(sz);
+    f.phiG.resize(sz);
+    if (int rc = mcv_get_state(p->h, slot, f.u.data(), f.v.data(), f.phi.data(), f.phiG.data())) return rc;
+    f.nsteps = p->total[slot];
+    f.finite = flags[slot] ? 0 : 1;
+    const long long id = p->req[slot];
+    s->finished[id] = std::move(f);
+    s->unreported.push_back(id);
+    p->req[slot] = -1;
+  }
+  p->active = still;
+  return MCV_OK;
+}
+
+int check_grid(int order, int nc, double dt, long long nsteps) {
+  if (order != 3 && order != 4) return fail(MCV_ERR_ARG, "order must be 3 (MCV3) or 4 (MCV4)");
+  if (nc < 2 || nc > 4096) return fail(MCV_ERR_ARG, "nc out of range [2, 4096]");
+  if (!(dt > 0.) || !std::isfinite(dt)) return fail(MCV_ERR_ARG, "dt must be positive and finite");
+  if (nsteps < 1) return fail(MCV_ERR_ARG, "nsteps must be >= 1");
+  return MCV_OK;
+}
+
+}  // namespace
+
+extern "C" int mcv_server_create(int precision, int scheme, double radius, long long hbm_budget,
+                                 long long slot_bytes, int max_slots, double chunk_ms, int tile, mcv_server **out) {
+  if (!out) return fail(MCV_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (precision != MCV_FP64 && precision != MCV_MIXED)
+    return fail(MCV_ERR_ARG, "precision must be MCV_FP64 or MCV_MIXED");
+  if (scheme != MCV_RK3_TVD && scheme != MCV_RK4) return fail(MCV_ERR_ARG, "scheme must be MCV_RK3_TVD or MCV_RK4");
+  if (!(radius > 0.) || !std::isfinite(radius)) return fail(MCV_ERR_ARG, "radius must be positive and finite");
+  if (slot_bytes < 1 || max_slots < 1) return fail(MCV_ERR_ARG, "slot_bytes and max_slots must be >= 1");
+  if (!(chunk_ms > 0.) || !std::isfinite(chunk_ms)) return fail(MCV_ERR_ARG, "chunk_ms must be positive");
+  if (tile < -1) return fail(MCV_ERR_ARG, "tile must be -1 (autotune) or a candidate index");
+  if (hbm_budget <= 0) {
+    long long free_b = 0, total_b = 0;
+    if (int rc = mcv_device_memory(&free_b, &total_b)) return rc;
+    hbm_budget = (long long)(0.85 * (double)free_b);
+  }
+  mcv_server *s = new mcv_server();
+  s->precision = precision;
+  s->scheme = scheme;
+  s->radius = radius;
+  s->budget = hbm_budget;
+  s->slot_bytes = slot_bytes;
+  s->max_slots = max_slots;
+  s->chunk_ms = chunk_ms;
+  s->tile = tile;
+  *out = s;
+  return MCV_OK;
+}
+
+extern "C" int mcv_server_submit(mcv_server *s, int order, int nc, double dt, long long nsteps, const double *phi_s,
+                                 const double *u, const double *v, const double *phi, long long *id) {
+  if (!s || !id) return fail(MCV_ERR_ARG, "server or id is NULL");
+  if (int rc = check_grid(order, nc, dt, nsteps)) return rc;
+  if (!phi_s || !u || !v || !phi) return fail(MCV_ERR_ARG, "state array is NULL");
+  if (footprint(s, order, nc, 1) > s->budget) return fail(MCV_ERR_NOMEM, "the request's grid exceeds the HBM budget");
+  int npx, n, halo;
+  mcv_grid_sizes(order, nc, &npx, &n, &halo);
+  const size_t sz = (size_t)npx * npx * 6;
+  Request r{};
+  r.id = s->next_id++;
+  r.order = order;
+  r.nc = nc;
+  r.dt = dt;
+  r.nsteps = nsteps;
+  r.spec = false;
+  r.phis.assign(phi_s, phi_s + sz);
+  r.u.assign(u, u + sz);
+  r.v.assign(v, v + sz);
+  r.phi.assign(phi, phi + sz);
+  s->waiting.push_back(std::move(r));
+  *id = s->next_id - 1;
+  return MCV_OK;
+}
+
+extern "C" int mcv_server_submit_balanced_flow(mcv_server *s, int order, int nc, double dt, long long nsteps,
+                                               double gh0, double u0, double alpha, int lmax, const double *coef,
+                                               double rms, double mountain_h0, double lon_c, double lat_c,
+                                               double efold, long long *id) {
+  if (!s || !id) return fail(MCV_ERR_ARG, "server or id is NULL");
+  if (int rc = check_grid(order, nc, dt, nsteps)) return rc;
+  if (lmax < 0 || lmax > 200 || (lmax > 0 && !coef)) return fail(MCV_ERR_ARG, "bad harmonic arguments");
+  if (mountain_h0 > 0. && !(efold > 0.)) return fail(MCV_ERR_ARG, "bad mountain arguments");
+  if (footprint(s, order, nc, 1) > s->budget) return fail(MCV_ERR_NOMEM, "the request's grid exceeds the HBM budget");
+  Request r{};
+  r.id = s->next_id++;
+  r.order = order;
+  r.nc = nc;
+  r.dt = dt;
+  r.nsteps = nsteps;
+  r.spec = true;
+  r.gh0 = gh0;
+  r.u0 = u0;
+  r.alpha = alpha;
+  r.lmax = lmax;
+  if (lmax > 0) r.coef.assign(coef, coef + (size_t)(lmax + 1) * (lmax + 1));
+  r.rms = rms;
+  r.mh0 = mountain_h0;
+  r.lon_c = lon_c;
+  r.lat_c = lat_c;
+  r.efold = efold;
+  s->waiting.push_back(std::move(r));
+  *id = s->next_id - 1;
+  return MCV_OK;
+}
+
+extern "C" int mcv_server_prepare(mcv_server *s, int order, int nc, double dt) {
+  if (!s) return fail(MCV_ERR_ARG, "server is NULL");
+  if (int rc = check_grid(order, nc, dt, 1)) return rc;
+  for (Pool *p : s->pools)
+    if (p->same_grid(order, nc, dt)) return MCV_OK;
+  int rc;
+  Pool *p = new_pool(s, order, nc, dt, &rc);
+  if (!p) return rc ? rc : fail(MCV_ERR_NOMEM, "the HBM budget has no room for the pool");
+  // a resting ocean in slot 0, stepped once: autotuning and graph capture
+  // happen here and not inside a request's latency
+  const int zero = 0;
+  if ((rc = mcv_set_member_balanced_flow(p->h, 0, 2.94e4, 0., 0., 0, nullptr, 0., 0., 0., 0., 0.)) ||
+      (rc = mcv_set_active(p->h, 1, &zero)) || (rc = mcv_step(p->h, 1)) || (rc = mcv_set_active(p->h, 0, nullptr)))
+    return rc;
+  p->dev_active.clear();
+  p->dev_active_set = true;
+  return MCV_OK;
+}
+
+extern "C" int mcv_server_poll(mcv_server *s, long long *ids, int max_ids, int *n_ids) {
+  if (!s || !n_ids || max_ids < 0 || (max_ids > 0 && !ids)) return fail(MCV_ERR_ARG, "bad poll arguments");
+  *n_ids = 0;
+  // 1. chunks that ended
+  for (Pool *p : s->pools) {
+    if (!p->in_flight) continue;
+    const int q = mcv_query(p->h);
+    if (q == MCV_BUSY) continue;
+    if (q != MCV_OK) return q;
+    if (int rc = finish_chunk(s, p)) return rc;
+  }
+  // 2. admission, first come first served among the requests that fit
+  for (auto it = s->waiting.begin(); it != s->waiting.end();) {
+    int placed;
+    if (int rc = admit(s, *it, &placed)) return rc;
+    it = placed ? s->waiting.erase(it) : std::next(it);
+  }
+  // 3. the next chunk of every idle pool with active slots
+  for (Pool *p : s->pools) {
+    if (p->in_flight || p->active.empty()) continue;
+    if (!p->dev_active_set || p->dev_active != p->active) {
+      if (int rc = mcv_set_active(p->h, (int)p->active.size(), p->active.data())) return rc;
+      p->dev_active = p->active;
+      p->dev_active_set = true;
+    }
+    const long long k = chunk_steps(s, p);
+    p->launched = now_ms();
+    if (int rc = mcv_step_async(p->h, (int)k)) return rc;
+    p->in_flight = k;
+  }
+  // 4. the forecasts finished since the last poll
+  while (*n_ids < max_ids && !s->unreported.empty()) {
+    ids[(*n_ids)++] = s->unreported.front();
+    s->unreported.pop_front();
+  }
+  return MCV_OK;
+}
+
+extern "C" int mcv_server_result(mcv_server *s, long long id, double *u, double *v, double *phi, double *phiG,
+                                 long long *nsteps, int *finite) {
+  if (!s) return fail(MCV_ERR_ARG, "server is NULL");
+  auto it = s->finished.find(id);
+  if (it == s->finished.end()) {
+    if (id >= 1 && id < s->next_id) {
+      bool queued = false;
+      for (const Request &r : s->waiting) queued = queued || r.id == id;
+      for (const Pool *p : s->pools)
+        for (long long r : p->req) queued = queued || r == id;
+      if (queued) return MCV_BUSY;
+    }
+    return fail(MCV_ERR_ARG, "no such request (unknown, or its result was already taken)");
+  }
+  const Finished &f = it->second;
+  const size_t bytes = f.u.size() * sizeof(double);
+  if (u) std::memcpy(u, f.u.data(), bytes);
+  if (v) std::memcpy(v, f.v.data(), bytes);
+  if (phi) std::memcpy(phi, f.phi.data(), bytes);
+  if (phiG) std::memcpy(phiG, f.phiG.data(), bytes);
+  if (nsteps) *nsteps = f.nsteps;
+  if (finite) *finite = f.finite;
+  s->finished.erase(it);
+  for (auto q = s->unreported.begin(); q != s->unreported.end(); ++q)
+    if (*q == id) {
+      s->unreported.erase(q);
+      break;
+    }
+  return MCV_OK;
+}
+
+extern "C" int mcv_server_stats(mcv_server *s, long long *stats) {
+  if (!s || !stats) return fail(MCV_ERR_ARG, "server or stats is NULL");
+  long long running = 0, busy = 0;
+  for (const Pool *p : s->pools) {
+    for (long long r : p->req) running += r >= 0;
+    busy += p->in_flight > 0;
+  }
+  stats[0] = (long long)s->waiting.size();
+  stats[1] = running;
+  stats[2] = (long long)s->finished.size();
+  stats[3] = (long long)s->pools.size();
+  stats[4] = busy;
+  stats[5] = used_bytes(s);
+  stats[6] = s->pools_created;
+  stats[7] = s->pools_evicted;
+  stats[8] = s->chunks;
+  return MCV_OK;
+}
+
+extern "C" int mcv_server_destroy(mcv_server *s) {
+  if (!s) return MCV_OK;
+  for (Pool *p : s->pools) close_pool(p);
+  delete s;
+  return MCV_OK;
+}

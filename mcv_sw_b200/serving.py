@@ -381,6 +381,47 @@ def run_one_at_a_time(requests, precision="fp64", scheme="RK3_TVD", radius=cases
     return [out[r.id] for r in requests]
 
 
+def run_native(requests, precision="mixed", scheme="RK3_TVD", radius=cases.EARTH_RADIUS, tile=-1, chunk_ms=25.0,
+               hbm_budget=0, slot_bytes=8e9, max_slots=32, keep_states=False, geoms=None, prepare=True,
+               poll_s=2e-4, clock=time.perf_counter):
+    """Serve `requests` with the native server (mcv_server_*): each request is
+    submitted at its arrival time, with the dt and step count ForecastServer
+    gives it, and the loop polls until every forecast is back.  Returns the
+    Results in input order (`admitted` is the submission time) and the
+    largest number of pools seen with a chunk on the GPU at once."""
+    policy = ForecastServer(precision=precision, scheme=scheme, hbm_budget=1 << 62, radius=radius, geoms=geoms)
+    results, by_id, busy_max = {}, {}, 0
+    with api.Server(precision, scheme, radius, int(hbm_budget), int(slot_bytes), max_slots, chunk_ms, tile) as srv:
+        if prepare:
+            for key in sorted({r.key for r in requests}):
+                srv.prepare(key[0], key[1], policy.group_dt(key))
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        t0 = clock()
+        while len(results) < len(requests):
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                r = pending.popleft()
+                n, dt = policy.nsteps(r), policy.group_dt(r.key)
+                if r.spec is not None:
+                    rid = srv.submit_spec(r.order, r.nc, dt, n, r.spec)
+                else:
+                    rid = srv.submit(r.order, r.nc, dt, n, r.phi_s, r.u, r.v, r.phi)
+                by_id[rid] = (r, now, dt)
+            done = srv.poll()
+            busy_max = max(busy_max, srv.stats()["busy_pools"])
+            for rid in done:
+                r, submitted, dt = by_id.pop(rid)
+                state, steps, finite = srv.result(rid)
+                results[r.id] = Result(r.id, r.order, r.nc, steps, dt, r.arrival, submitted, clock() - t0,
+                                       finite=finite, state=state if keep_states else None)
+            if not done:
+                if not by_id and pending:
+                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (clock() - t0))))
+                else:
+                    time.sleep(poll_s)
+    return [results[r.id] for r in requests], busy_max
+
+
 def summarize(results):
     lat = np.array([r.latency for r in results])
     days = sum(r.sim_days for r in results)

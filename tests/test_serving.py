@@ -2,10 +2,12 @@
 reuse, eviction) with a stand-in for the device handle: each member's "state"
 counts the steps it was advanced, so a forecast that is stepped too far or
 too little shows up exactly."""
+import os
+
 import numpy as np
 import pytest
 
-from mcv_sw_b200 import serving
+from mcv_sw_b200 import api, serving
 
 
 class FakeStepper:
@@ -176,3 +178,49 @@ def test_device_setup_admits_spec_requests():
         assert r.state["seed"] == q.spec["marker"]
         assert r.state["steps"] == r.nsteps == srv.nsteps(q)
     assert all(getattr(st, "device_geometry", False) for st in FakeStepper.created)
+
+
+def test_native_server_arguments_and_queue():
+    """mcv_server_*: argument checks and the request queue, before any device
+    call (admission, which creates pools, happens only in mcv_server_poll)."""
+    L = api.lib()
+    with pytest.raises(api.MCVError) as e:
+        api.Server("fp64", hbm_budget=1 << 30, chunk_ms=0.0)
+    assert e.value.code == -1
+    with pytest.raises(api.MCVError) as e:
+        api.Server("fp64", hbm_budget=1 << 30, tile=-2)
+    assert e.value.code == -1
+    with api.Server("fp64", hbm_budget=1 << 30) as srv:
+        assert srv.poll() == []
+        npx, _, _ = api.grid_sizes(3, 4)
+        z = np.zeros((6, npx, npx))
+        for order, nc, dt, n in ((3, 1, 100.0, 1), (3, 4, -1.0, 1), (3, 4, float("nan"), 1), (3, 4, 100.0, 0)):
+            with pytest.raises(api.MCVError) as e:
+                srv.submit(order, nc, dt, n, z, z, z, z)
+            assert e.value.code == -1
+        with pytest.raises(ValueError):
+            srv.submit(3, 4, 100.0, 1, z[:3], z, z, z)
+        assert srv.submit(3, 4, 100.0, 2, z, z, z, z) == 1
+        assert srv.submit_spec(4, 4, 50.0, 3, {"gh0": 2.94e4, "u0": 10.0, "alpha": 0.0, "lmax": 0, "rms": 0.0,
+                                                "coef": None, "mountain": None}) == 2
+        st = srv.stats()
+        assert (st["waiting"], st["running"], st["pools"], st["pool_bytes"]) == (2, 0, 0, 0)
+        assert srv.result(1) is None  # queued
+        assert L.mcv_server_result(srv.s, 99, None, None, None, None, None, None) == -1
+        assert L.mcv_server_submit_balanced_flow(srv.s, 3, 4, 100.0, 1, 2.94e4, 0.0, 0.0, 2, None, 1.0, 0.0, 0.0,
+                                                 0.0, 0.0, None) == -1
+    with api.Server("fp64", hbm_budget=1000) as tiny:
+        with pytest.raises(api.MCVError) as e:
+            tiny.submit(3, 4, 100.0, 1, z, z, z, z)
+        assert e.value.code == -3  # even a one-slot pool exceeds the budget
+
+
+@pytest.mark.skipif(os.path.exists("/dev/nvidia0"), reason="checks the no-GPU behaviour")
+def test_native_server_has_no_cpu_path():
+    npx, _, _ = api.grid_sizes(3, 4)
+    z = np.zeros((6, npx, npx))
+    with api.Server("fp64", hbm_budget=1 << 30) as srv:
+        srv.submit(3, 4, 100.0, 2, z, z, z, z)
+        with pytest.raises(api.MCVError) as e:
+            srv.poll()  # admission creates the pool's handle
+        assert e.value.code == -2

@@ -106,6 +106,28 @@ def test_inactive_members_keep_their_state():
             assert s.query()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_native_server_matches_the_request_loop(precision):
+    """mcv_server_* against ForecastServer with device geometry, on host-array
+    and device-generated requests: the same forecasts bit for bit, with pools
+    of different grids on the GPU at once."""
+    reqs, geoms = stream()
+    rng = np.random.default_rng(5)
+    for i, (order, nc, hours) in enumerate([(4, 8, 2.0), (3, 12, 1.0)]):
+        spec = cases.balanced_flow_spec(cases._Radius(cases.EARTH_RADIUS), rng, lmax=4, mountain=bool(i))
+        reqs.append(serving.Request(len(reqs), 0.003 * i, order, nc, hours, spec=spec))
+    kw = dict(precision=precision, tile=0, keep_states=True, geoms=geoms, hbm_budget=4 << 30, slot_bytes=64 << 20,
+              chunk_ms=0.5)
+    py = serving.ForecastServer(device_setup=True, **kw)
+    a = py.run(reqs)
+    py.close()
+    b, busy = serving.run_native(reqs, **kw)
+    assert busy >= 2
+    for req, x, y in zip(reqs, a, b):
+        assert y.finite and x.nsteps == y.nsteps
+        assert same(x, y), req.id
+
+
 def test_device_admission_stream():
     """Requests carrying seeded specs, admitted by generating their states on
     the device into pools whose geometry was built there: each result is the
