@@ -45,9 +45,14 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=20)
     p.add_argument("--ensemble", type=int, default=1, help="run the 64-member ensemble block (1 GPU only)")
-    p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving block (0: skip)")
+    p.add_argument("--serve-requests", type=int, default=200,
+                   help="requests of the serving stream served by both continuous-batching loops (0: skip)")
+    p.add_argument("--serve-baseline-requests", type=int, default=24,
+                   help="first requests of the stream also run by the FP64 one-request-at-a-time loop")
     p.add_argument("--stress", type=int, default=1, help="run the Nc=1024 roofline-stress block (1 GPU only)")
     p.add_argument("--admission", type=int, default=1, help="run the device-admission timing block (1 GPU only)")
+    p.add_argument("--paths", default="fp64,mixed",
+                   help="precisions timed on the main workload (the headline precision must be one of them)")
     p.add_argument("--tiles", default=None,
                    help="pin the stage-kernel candidates of the main workload as 'fp64_index,mixed_index' "
                         "(default: each handle's autotuner chooses)")
@@ -196,15 +201,28 @@ def cpu_baseline(st, budget_s=20.0):
             "sample": f"{nsteps} RK steps of the same workload after 1 warm-up step ({el:.1f} s)"}
 
 
+def mapped_libraries():
+    """Shared objects mapped into this process (from /proc/self/maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return sorted({line.split()[-1] for line in f if line.rstrip().endswith(".so") or ".so." in line})
+    except OSError:
+        return []
+
+
 def run_reference(args):
+    """The reference algorithm's CPU implementation (the FP64 oracle, all host
+    threads) on the same workload, built from the oracle's own mesh and IC
+    routines: this arm maps no GPU library of the product."""
     world, rank, local = dist_setup()
     if rank != 0:
         return
-    st, geom, desc = build_workload(args.workload)
     from oracle import oracle as orc
-    o = orc.Oracle(st.order, st.nc, st.dt, st.scheme, 6.371e6)
-    o.set_phi_s(st.phi_s)
-    o.init_state(st.zonal, st.merid, st.phi)
+    from oracle import workloads
+    w, desc = workloads.build(args.workload)
+    if any("libmcv_gpu" in m for m in mapped_libraries()):
+        raise RuntimeError("the reference arm must not load the GPU library")
+    o = w.o
     o.step(min(args.warmup, 2))
     # bounded sample: at most args.steps RK steps or ~90 s of CPU time
     done, t0 = 0, time.perf_counter()
@@ -212,16 +230,18 @@ def run_reference(args):
         o.step(1)
         done += 1
     el = time.perf_counter() - t0
-    value = done * st.dt / 86400.0 / el
+    value = done * w.dt / 86400.0 / el
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": done, "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * el / done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": desc, "order": st.order, "nc": st.nc, "scheme": st.scheme,
-                                            "precision": "fp64", "dt_s": st.dt},
+            "data": "synthetic", "config": {"workload": desc, "order": w.order, "nc": w.nc, "scheme": w.scheme,
+                                            "precision": "fp64", "dt_s": w.dt},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
                              "sample": f"{done} RK steps (of {args.steps} asked; capped at ~90 s) after "
-                                       f"{min(args.warmup, 2)} warm-up steps"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                                       f"{min(args.warmup, 2)} warm-up steps; inputs built by the oracle "
+                                       f"(oracle/workloads.py), no GPU library mapped"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "libraries": [m for m in mapped_libraries() if "oracle" in m or "mcv" in m]}
     print(json.dumps(line), flush=True)
 
 
@@ -295,23 +315,34 @@ def ensemble_block(steps=40, days=2.0, members=64):
     return out
 
 
-def serving_block(count):
-    """The serving stream's first `count` requests through the continuous-batching
-    server (split precision) and through the plain FP64 one-request-at-a-time loop."""
+def serving_block(count, baseline_count):
+    """The serving stream's first `count` requests through both continuous-batching
+    loops in split precision -- the native request loop behind the C ABI
+    (mcv_server_*, what a C or Fortran driver calls) and the Python loop over
+    the per-handle calls -- and its first `baseline_count` requests through the
+    plain FP64 one-request-at-a-time loop.  The stream (Poisson arrivals at 20
+    req/s) asks for far more simulated days per second than one GPU delivers,
+    so latencies include the backlog that builds up over the stream."""
     from mcv_sw_b200 import serving
     reqs, geoms = serving.make_requests(count, specs=True)
     keys = sorted({r.key for r in reqs})
+    out = {"requests": count,
+           "stream": "Poisson 20 req/s (seed 4), MCV3/MCV4 50/50, Nc 48/96/192/384 (.4/.3/.2/.1), 6-120 h, half "
+                     "with mountains; RK3_TVD, CFL 0.45; geometry and initial states generated on the device at "
+                     "admission"}
+    res, busy = serving.run_native(reqs, precision="mixed", geoms=geoms)
+    out["native_server_mixed"] = dict(serving.summarize(res), max_concurrent_pools=busy,
+                                      loop="mcv_server_submit_balanced_flow / mcv_server_poll / mcv_server_result")
     srv = serving.ForecastServer(precision="mixed", geoms=geoms, device_setup=True)
     srv.prepare(keys)
     res = srv.run(reqs)
-    stats = dict(srv.stats)
+    out["python_server_mixed"] = dict(serving.summarize(res), **srv.stats)
     srv.close()
-    base = serving.run_one_at_a_time(reqs, precision="fp64", geoms=geoms, device_setup=True)
-    return {"requests": count, "stream": "Poisson 20 req/s (seed 4), MCV3/MCV4 50/50, Nc 48/96/192/384 "
-                                         "(.4/.3/.2/.1), 6-120 h, half with mountains; RK3_TVD, CFL 0.45; "
-                                         "geometry and initial states generated on the device at admission",
-            "server_mixed": serving.summarize(res), "server_stats": stats,
-            "one_at_a_time_fp64": serving.summarize(base)}
+    if baseline_count > 0:
+        base = serving.run_one_at_a_time(reqs[:baseline_count], precision="fp64", geoms=geoms, device_setup=True)
+        out["one_at_a_time_fp64"] = serving.summarize(base)
+        out["one_at_a_time_fp64"]["note"] = f"the stream's first {baseline_count} requests"
+    return out
 
 
 def stress_block(steps=200):
@@ -386,7 +417,10 @@ def run_ours(args):
             dist.barrier()
 
     paths = {}
-    for precision in ("fp64", "mixed"):
+    timed = [x for x in ("fp64", "mixed") if x in args.paths.split(",")]
+    if args.precision not in timed:
+        raise SystemExit("--paths must include the headline --precision")
+    for precision in timed:
         s, paths[precision] = time_path(args, st, geom, precision, world, barrier, dist, local)
         if precision != args.precision:
             s.close()
@@ -410,22 +444,24 @@ def run_ours(args):
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     hp = {k: pin(getattr(st, k)) for k in ("phi_s", "u", "v", "phi")}
     ho = {k: torch.empty(geom.shape, dtype=torch.float64).pin_memory().numpy() for k in ("u", "v", "phi")}
-    main.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
-    main.step(1)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        main.set_state(0, hp["u"], hp["v"], hp["phi"])
+    e2e = None
+    if args.e2e_steps > 0:
+        main.set_member(0, hp["phi_s"], hp["u"], hp["v"], hp["phi"])
         main.step(1)
-        main.get_state(0, out=ho)
-    barrier()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, dist)
-    field_bytes = 8 * 6 * geom.npx * geom.npx
-    e2e = {"value": world * args.e2e_steps * st.dt / 86400.0 / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": 3 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
-           "how": "per step: mcv_set_state (u, v, phi from pinned host) + mcv_step(1) + "
-                  "mcv_get_state (u, v, phi to pinned host); host wall clock around synchronous calls"}
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            main.set_state(0, hp["u"], hp["v"], hp["phi"])
+            main.step(1)
+            main.get_state(0, out=ho)
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s, dist)
+        field_bytes = 8 * 6 * geom.npx * geom.npx
+        e2e = {"value": world * args.e2e_steps * st.dt / 86400.0 / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": 3 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
+               "how": "per step: mcv_set_state (u, v, phi from pinned host) + mcv_step(1) + "
+                      "mcv_get_state (u, v, phi to pinned host); host wall clock around synchronous calls"}
     main.close()
 
     # accuracy of split precision against the FP64 path over the full forecast,
@@ -480,7 +516,7 @@ def run_ours(args):
         if args.ensemble:
             extra["ensemble"] = ensemble_block()
         if args.serve_requests > 0:
-            extra["serving"] = serving_block(args.serve_requests)
+            extra["serving"] = serving_block(args.serve_requests, args.serve_baseline_requests)
         if args.stress:
             extra["stress"] = stress_block()
         if args.admission:
@@ -497,8 +533,12 @@ def run_ours(args):
                            "l2": "no flush: each stage reads > 126 MB (inputs larger than L2)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": args.steps * 2 * nst, "clocks": head["clocks"],
-                "paths": {"fp64": paths["fp64"], "mixed": paths["mixed"]},
-                f"speedup_{args.precision}_vs_{other}": head["value"] / paths[other]["value"],
+                "paths": paths,
+                f"speedup_{args.precision}_vs_{other}": (head["value"] / paths[other]["value"]
+                                                         if other in paths else None),
+                # like for like: the FP64 GPU path against the FP64 CPU oracle on the same box
+                "fp64_gpu_vs_cpu_baseline": (paths["fp64"]["value"] / cpu["value"]
+                                             if cpu and "fp64" in paths else None),
                 "accuracy": accuracy, **extra}
         print(json.dumps(line), flush=True)
     if dist is not None:

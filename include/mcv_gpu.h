@@ -6,7 +6,8 @@
  *   RK3_TVD(stat(new), stat(old))   src/time_scheme_mod.F90:46-69
  * from src/MCV_SW.F90:57-60, on module-global arrays.  This header is the
  * drop-in boundary for that loop: a Fortran driver binds it with
- * iso_c_binding, Python binds it with ctypes.
+ * iso_c_binding (an interface module of bind(C) declarations mirroring the
+ * prototypes below), Python binds it with ctypes.
  *
  * Conventions
  *  - Every function returns an int status: 0 = OK, < 0 = error;
@@ -158,6 +159,37 @@ int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double *phi, doubl
  * device in FP64 with compensated (Neumaier) summation. */
 int mcv_mass_energy(mcv_handle *h, int m, double *mass, double *energy);
 
+/* History-output staging: the sequence the reference's time loop runs at a
+ * history interval (src/MCV_SW.F90:62-67) on member m's device state, with
+ * only the requested outputs crossing PCIe (any pointer may be NULL):
+ *  - u, v, phi over the padded range with FillValue in the halo corner
+ *    squares of u and v (addFillValue, src/output_mod.F90:230-248) and of phi
+ *    once a step has run (src/ghost_mod.f90:161,179);
+ *  - zonal, merid: convert_wind_P2SP over the whole padded range
+ *    (src/spatial_operators_mod.F90:391-405) of those u, v, with A IG
+ *    evaluated per point on the device from the equiangular formulas at the
+ *    handle's radius (which must be the geometry's);
+ *  - uC, vC, phiC: calc_VIA (src/diag_mod.F90:69-93) of u, v, phi with the
+ *    reference's weightsOnPV (MCV4's /80 included, src/mesh_mod.F90:183-203),
+ *    in stat%uC's layout (ics:ice, jcs:jce, 6) = (nc+2, nc+2, 6), halo cells 0.
+ * A Fortran driver passes stat(new)'s arrays and calls history_write_stat
+ * unchanged; calc_total_mass / calc_total_energy are mcv_mass_energy. */
+int mcv_get_history(mcv_handle *h, int m, double *u, double *v, double *phi, double *zonal, double *merid,
+                    double *uC, double *vC, double *phiC);
+
+/* Normalized L1, L2 and Linf errors of doc/orderCheck.m:63-81 between the
+ * calc_VIA cell averages of phi of member ma of handle a and member mb of
+ * handle b (the reference), weighted by areaCell, computed on the device:
+ * norms[0..2] = L1, L2, Linf.  Both handles hold the same grid on the same
+ * device; b's queued work is waited for.  No reference counterpart (the
+ * reference computes these offline in MATLAB from its history files). */
+int mcv_height_error_norms(mcv_handle *a, int ma, mcv_handle *b, int mb, double *norms);
+
+/* mesh%areaCell (src/mesh_mod.F90:205-212, EquiangularAllAreas :240-276):
+ * cell areas in (ics:ice, jcs:jce, 6) = (nc+2, nc+2, 6) layout, halo cells 0.
+ * Host only. */
+int mcv_cell_areas(int nc, double radius, double *areaCell);
+
 /* Instrumentation (no counterpart in the reference, which only prints its
  * total wall time, src/MCV_SW.F90:80-82).
  * mcv_time_steps: advance nsteps and return their device time (CUDA events on
@@ -199,8 +231,10 @@ int mcv_select_tile(mcv_handle *h, int index);
  * waits for its own work.  Limits: members <= 64.  The scratch (one partial sum
  * per block and member) is a fixed static device array of about 300 KiB held by
  * every device that loads the library; the first call on a device looks up its
- * address, so make that first call before any stream capture.  Calls that
- * overlap on the GPU share the scratch and race. */
+ * address, so make that first call before any stream capture.  The address is
+ * kept per device and context: after a device reset (a new primary context)
+ * the next call looks it up again.  Calls that overlap on the GPU share the
+ * scratch and race. */
 int mcv_mass_energy_noalloc(int order, int nc, int members, const double *u, const double *v, const double *phi,
                             const double *phi_s, const double *sqrtG, const double *matrixIG, void *stream,
                             double *mass, double *energy);
@@ -234,7 +268,8 @@ typedef struct mcv_server mcv_server;
 
 /* precision, scheme, radius: as mcv_create, for every pool.  hbm_budget:
  * bytes the pools may hold (<= 0: 85% of the device's free memory now).  A
- * pool gets as many slots as fit in slot_bytes (1..max_slots).  chunk_ms: GPU
+ * pool gets as many slots as fit in slot_bytes (1..max_slots), fewer when the
+ * budget left by the pools in use holds fewer.  chunk_ms: GPU
  * time of one chunk, which bounds how long a request waits for a busy pool of
  * its grid.  tile: stage-kernel candidate of every pool (mcv_select_tile), or
  * -1 for each pool's autotuner. */
@@ -265,12 +300,16 @@ int mcv_server_prepare(mcv_server *s, int order, int nc, double dt);
  * queues the next chunk of every idle pool.  Writes up to max_ids ids of
  * forecasts finished since the last poll to ids (*n_ids of them); the rest
  * are reported by later polls.  A pool's first chunk autotunes its stage
- * kernel and captures its step graphs, which blocks (see mcv_server_prepare). */
+ * kernel and captures its step graphs, which blocks (see mcv_server_prepare).
+ * A forecast whose initial state, step or read-back fails is retired as
+ * failed and reported with the finished ids (its mcv_server_result returns the
+ * error); the poll returns the first such error and the loop goes on. */
 int mcv_server_poll(mcv_server *s, long long *ids, int max_ids, int *n_ids);
 
 /* Copy out and release a finished forecast: u, v, phi, phiG over the padded
  * range (any pointer may be NULL), its step count and *finite = 0 if its
- * state holds a NaN or Inf.  MCV_BUSY if it is still queued or running. */
+ * state holds a NaN or Inf.  MCV_BUSY if it is still queued or running; the
+ * forecast's error (and release) if it failed. */
 int mcv_server_result(mcv_server *s, long long id, double *u, double *v, double *phi, double *phiG,
                       long long *nsteps, int *finite);
 

@@ -69,6 +69,9 @@ def lib():
         "mcv_selftest_wait": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _I, _D]),
         "mcv_get_state": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
         "mcv_mass_energy": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
+        "mcv_get_history": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D]),
+        "mcv_height_error_norms": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, _D]),
+        "mcv_cell_areas": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
         "mcv_destroy": (ctypes.c_int, [vp]),
         "mcv_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _D]),
         "mcv_profile_step": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
@@ -193,6 +196,13 @@ class Geometry:
         for c in range(self.nc):
             line[self.H + c * (D - 1): self.H + c * (D - 1) + D] += w1
         return np.broadcast_to(np.outer(line, line), self.shape)
+
+
+def cell_areas(nc, radius):
+    """mesh%areaCell: (6, nc+2, nc+2) with zero halo cells."""
+    out = np.empty((6, nc + 2, nc + 2))
+    _check(lib().mcv_cell_areas(int(nc), float(radius), _dp(out)))
+    return out
 
 
 def selftest_wait(complete, limit_ms):
@@ -398,6 +408,24 @@ class Stepper:
         ms, en = ctypes.c_double(), ctypes.c_double()
         _check(lib().mcv_mass_energy(self.h, int(m), ctypes.byref(ms), ctypes.byref(en)))
         return ms.value, en.value
+
+    def get_history(self, m=0, fields=("u", "v", "phi", "zonal", "merid", "uC", "vC", "phiC")):
+        """mcv_get_history: the reference's history-output sequence on member m
+        (addFillValue, convert_wind_P2SP, calc_VIA of u, v, phi) formed on the
+        device.  Padded fields have shape (6, npx, npx), cell fields
+        (6, nc+2, nc+2) with zero halo cells."""
+        cell = (6, self.nc + 2, self.nc + 2)
+        names = ("u", "v", "phi", "zonal", "merid", "uC", "vC", "phiC")
+        out = {k: np.empty(cell if k.endswith("C") else (6, self.npx, self.npx)) for k in fields}
+        _check(lib().mcv_get_history(self.h, int(m), *[_dp(out.get(k)) for k in names]))
+        return out
+
+    def height_error_norms(self, m, ref, ref_m=0):
+        """(L1, L2, Linf) of member m's phi against member ref_m of Stepper
+        `ref`, on calc_VIA cell averages weighted by areaCell (orderCheck.m)."""
+        out = (ctypes.c_double * 3)()
+        _check(lib().mcv_height_error_norms(self.h, int(m), ref.h, int(ref_m), out))
+        return tuple(out)
 
 
 SERVER_STATS = ("waiting", "running", "unclaimed", "pools", "busy_pools", "pool_bytes", "pools_created",

@@ -11,7 +11,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 SOURCES = ["mcv_gpu.cu", "stage_d3_f64.cu", "stage_d3_mix.cu", "stage_d4_f64.cu", "stage_d4_mix.cu",
-           "mcv_geometry.cu", "mcv_noalloc.cu", "host_setup.cpp", "mcv_server.cpp"]
+           "mcv_geometry.cu", "mcv_diag.cu", "mcv_noalloc.cu", "host_setup.cpp", "mcv_server.cpp"]
 # per-source flags: the device geometry restates host formulas compiled
 # without FMA contraction
 SOURCE_FLAGS = {"mcv_geometry.cu": ["-fmad=false"]}

@@ -337,7 +337,32 @@ __global__ void ic_fields_kernel(const IcArgs a) {
   if (a.phis32) a.phis32[o] = (float)phs;
 }
 
+// convert_wind_P2SP (src/spatial_operators_mod.F90:391-405) over the padded
+// points after addFillValue (src/output_mod.F90:230-248): the halo corner
+// squares of u and v hold FillValue, and every point gets
+// (zonal, meridional) = (A IG)(u, v) with matmul's k = 1, 2 order
+// (covProjPlane2Sphere, src/projection_mod.F90:79-96).
+__global__ void history_p2sp_kernel(const GeomArgs a, const double *u, const double *v, int which, double *out) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x, jj = blockIdx.y, p = blockIdx.z;
+  if (ii >= a.npx) return;
+  PointGeo g;
+  point_geo(p + 1, coord(a, ii), coord(a, jj), a, g);
+  const bool corner = (ii < a.H || ii >= a.npx - a.H) && (jj < a.H || jj >= a.npx - a.H);
+  const long long o = ((long long)p * a.npx + jj) * a.P + ii;
+  const double fill = -9999999999999999.;  // FillValue, src/constants_mod.F90:20
+  const double cu = corner ? fill : u[o], cv = corner ? fill : v[o];
+  double m[4];
+  matmul22(m, g.A, g.IG);
+  out[((long long)p * a.npx + jj) * a.npx + ii] = which == 0 ? m[0] * cu + m[2] * cv : m[1] * cu + m[3] * cv;
+}
+
 }  // namespace
+
+int history_p2sp_device(const GeomArgs &a, const double *u, const double *v, int which, double *out,
+                        cudaStream_t s) {
+  history_p2sp_kernel<<<dim3((a.npx + 127) / 128, a.npx, 6), 128, 0, s>>>(a, u, v, which, out);
+  return (int)cudaGetLastError();
+}
 
 int ic_harmonics_device(const IcArgs &a, cudaStream_t s) {
   const int T = 128;

@@ -143,6 +143,7 @@ struct mcv_handle {
   int *flags = nullptr;  // non-finite flags [members]
   int *err = nullptr;    // stage-kernel error flag (TMA staging timed out)
   double *stage = nullptr;  // one FP64 field in the host's dense layout (PCIe copies land here)
+  double *area = nullptr;   // areaCell of one panel [nc][nc] (the error norms' weights)
   int nsm = 0;           // SMs of the device
   std::vector<int> bps;  // resident CTAs per SM of each candidate
   int launch_err = 0;    // status of the last stage launch (tensor-map encoding)
@@ -174,7 +175,7 @@ struct Layout {
   size_t total = 0;
   size_t f64_state[9]{}, f64_acc[3]{}, mix_state[6]{}, mix_inc[6]{}, mix_acc[3]{};
   size_t metric[5]{}, phis = 0, phis32 = 0, bnd = 0, bnd32 = 0, M = 0, N = 0, iref = 0, coef = 0, partial = 0,
-         met1d = 0, phibar = 0, active = 0, flags = 0, err = 0, stage = 0, prec = 0;
+         met1d = 0, phibar = 0, active = 0, flags = 0, err = 0, stage = 0, prec = 0, area = 0;
 };
 
 Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int members) {
@@ -221,6 +222,7 @@ Layout make_layout(const GridDesc &g, int H, int scheme, int precision, int memb
   L.flags = take(sizeof(int) * (size_t)members);
   L.err = take(sizeof(int));
   L.stage = take(sizeof(double) * 6 * (size_t)g.np * g.np);  // one dense host-layout FP64 field
+  L.area = take(sizeof(double) * (size_t)g.Nc * g.Nc);         // areaCell of one panel
   L.total = off;
   return L;
 }
@@ -696,8 +698,13 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->flags = (int *)(base + L.flags);
   h->err = (int *)(base + L.err);
   h->stage = (double *)(base + L.stage);
+  h->area = (double *)(base + L.area);
   // zero everything once: unused pitch padding and halo corners stay finite
   e = cudaMemsetAsync(h->pool, 0, L.total, h->stream);
+  std::vector<double> area((size_t)nc * nc);
+  equiangular_cell_areas(nc, radius, area.data());
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h->area, area.data(), sizeof(double) * area.size(), cudaMemcpyHostToDevice, h->stream);
   // every member is active until mcv_set_active says otherwise
   h->active_host.resize(members);
   for (int m = 0; m < members; ++m) h->active_host[m] = m;
@@ -1274,6 +1281,142 @@ extern "C" int mcv_mass_energy(mcv_handle *h, int m, double *mass, double *energ
   }
   if (mass) *mass = ms.s + ms.c;
   if (energy) *energy = es.s + es.c;
+  return MCV_OK;
+}
+
+namespace {
+
+// The equiangular sqrtG of the handle's radius at the middle padded point of
+// panel 1 agrees with the geometry the handle holds (device formulas that
+// take the radius -- the history's A IG -- need the caller's radius).
+bool radius_matches(const mcv_handle *h) {
+  const int npx = h->npx, mid = npx / 2;
+  const double pi = 2.0 * std::asin(1.0);
+  const double x = (double)(mid + (1 - h->H) - 1) * h->g.dx / (double)(h->order - 1) + (-45. * pi / 180.);
+  const double t = std::tan(x), c = std::cos(x);
+  const double rho2 = 1. + 2. * t * t;
+  const double sg = h->radius * h->radius / (c * c * c * c * rho2 * std::sqrt(rho2));
+  const size_t k = (size_t)mid + (size_t)npx * mid;
+  return k < h->sqrtG_host.size() && std::fabs(h->sqrtG_host[k] / sg - 1.) <= 1e-9;
+}
+
+GeomArgs history_args(const mcv_handle *h) {
+  GeomArgs a{};
+  a.order = h->order;
+  a.nc = h->nc;
+  a.npx = h->npx;
+  a.n = h->g.n;
+  a.H = h->H;
+  a.P = h->g.P;
+  a.radius = h->radius;
+  a.dx = h->g.dx;
+  a.pi = 2.0 * std::asin(1.0);
+  a.x_min = -45. * (a.pi / 180.);
+  return a;
+}
+
+// FillValue (src/constants_mod.F90:20) in the four H x H halo corner squares
+// of a padded host field of the handle's grid.
+void fill_corners(const mcv_handle *h, double *fld) {
+  const int npx = h->npx, H = h->H;
+  for (int p = 0; p < 6; ++p)
+    for (int cj = 0; cj < 2; ++cj)
+      for (int ci = 0; ci < 2; ++ci)
+        for (int j = 0; j < H; ++j)
+          for (int i = 0; i < H; ++i) {
+            const size_t ii = ci ? (size_t)(npx - H + i) : (size_t)i, jj = cj ? (size_t)(npx - H + j) : (size_t)j;
+            fld[ii + (size_t)npx * (jj + (size_t)npx * p)] = -9999999999999999.;
+          }
+}
+
+}  // namespace
+
+extern "C" int mcv_get_history(mcv_handle *h, int m, double *u, double *v, double *phi, double *zonal, double *merid,
+                               double *uC, double *vC, double *phiC) {
+  if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+  if (m < 0 || m >= h->members) return fail(MCV_ERR_ARG, "member index out of range");
+  if (!h->geometry_set || !h->member_set[m]) return fail(MCV_ERR_ORDER, "geometry and member must be set");
+  if ((zonal || merid) && !radius_matches(h))
+    return fail(MCV_ERR_ARG, "the handle's radius does not match its geometry (the wind rotation needs it)");
+  const long long off = (long long)m * h->g.mstride;
+  double *const *Y = state(h, m);
+  const size_t field = (size_t)h->npx * h->npx * 6 * sizeof(double);
+  int rc;
+  if (u && (rc = download_padded(h, u, Y[0] + off))) return rc;
+  if (v && (rc = download_padded(h, v, Y[1] + off))) return rc;
+  if (phi && (rc = download_padded(h, phi, Y[2] + off))) return rc;
+  const GeomArgs ga = history_args(h);
+  double *const wind[2] = {zonal, merid};
+  for (int which = 0; which < 2; ++which) {
+    if (!wind[which]) continue;
+    // the staging field is free again once the previous copy out has run
+    if (int e = history_p2sp_device(ga, Y[0] + off, Y[1] + off, which, h->stage, h->stream))
+      return cuda_fail((cudaError_t)e, "history wind rotation");
+    MCV_CUDA(cudaMemcpyAsync(wind[which], h->stage, field, cudaMemcpyDeviceToHost, h->stream), "download wind");
+  }
+  double *const cells[3] = {uC, vC, phiC};
+  const size_t ncell = (size_t)(h->nc + 2) * (h->nc + 2) * 6;
+  for (int f = 0; f < 3; ++f) {
+    if (!cells[f]) continue;
+    if (int e = via_device(h->order, h->nc, h->npx, h->g.P, Y[f] + off, h->stage, h->stream))
+      return cuda_fail((cudaError_t)e, "cell averages");
+    MCV_CUDA(cudaMemcpyAsync(cells[f], h->stage, ncell * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+             "download cell averages");
+  }
+  MCV_CUDA(cudaStreamSynchronize(h->stream), "history download");
+  // addFillValue (output_mod.F90:230-248) on u, v; phi's corners hold FillValue
+  // once a step's correct_bdy_ghost has run (ghost_mod.f90:161,179)
+  if (u) fill_corners(h, u);
+  if (v) fill_corners(h, v);
+  if (phi && h->steps_done[m] > 0) fill_corners(h, phi);
+  return MCV_OK;
+}
+
+extern "C" int mcv_height_error_norms(mcv_handle *a, int ma, mcv_handle *b, int mb, double *norms) {
+  if (!a || !b || !norms) return fail(MCV_ERR_ARG, "handle or output is NULL");
+  if (ma < 0 || ma >= a->members || mb < 0 || mb >= b->members) return fail(MCV_ERR_ARG, "member index out of range");
+  if (a->order != b->order || a->nc != b->nc) return fail(MCV_ERR_ARG, "the two handles hold different grids");
+  if (a->device != b->device) return fail(MCV_ERR_ARG, "the two handles live on different devices");
+  if (!a->member_set[ma] || !b->member_set[mb]) return fail(MCV_ERR_ORDER, "both members must be set");
+  // b's queued steps come first
+  if (a != b) MCV_CUDA(cudaStreamSynchronize(b->stream), "wait for the reference handle");
+  const double *pa = state(a, ma)[2] + (long long)ma * a->g.mstride;
+  const double *pb = state(b, mb)[2] + (long long)mb * b->g.mstride;
+  const int blocks = kPartialBlocks / 2;
+  if (int e = norms_device(a->order, a->nc, a->npx, a->g.P, pa, pb, a->area, a->partial, blocks, a->stream))
+    return cuda_fail((cudaError_t)e, "error norms");
+  std::vector<double4> part(kPartialBlocks);
+  MCV_CUDA(cudaMemcpyAsync(part.data(), a->partial, sizeof(double4) * kPartialBlocks, cudaMemcpyDeviceToHost,
+                           a->stream),
+           "download norm partials");
+  MCV_CUDA(cudaStreamSynchronize(a->stream), "error norms");
+  double l1 = 0., r1 = 0., l2 = 0., r2 = 0., md = 0., mbx = 0.;
+  for (int k = 0; k < blocks; ++k) {
+    l1 += part[2 * k].x;
+    r1 += part[2 * k].y;
+    l2 += part[2 * k].z;
+    r2 += part[2 * k].w;
+    md = std::max(md, part[2 * k + 1].x);
+    mbx = std::max(mbx, part[2 * k + 1].y);
+  }
+  norms[0] = l1 / r1;
+  norms[1] = std::sqrt(l2 / r2);
+  norms[2] = md / mbx;
+  return MCV_OK;
+}
+
+extern "C" int mcv_cell_areas(int nc, double radius, double *areaCell) {
+  if (nc < 2 || nc > 4096 || !(radius > 0.) || !areaCell) return fail(MCV_ERR_ARG, "bad cell-area arguments");
+  std::vector<double> a((size_t)nc * nc);
+  equiangular_cell_areas(nc, radius, a.data());
+  const int nce = nc + 2;
+  for (int p = 0; p < 6; ++p)
+    for (int j = 0; j < nce; ++j)
+      for (int i = 0; i < nce; ++i) {
+        const bool in = i >= 1 && i <= nc && j >= 1 && j <= nc;
+        areaCell[(size_t)i + (size_t)nce * ((size_t)j + (size_t)nce * p)] =
+            in ? a[(size_t)(i - 1) + (size_t)nc * (j - 1)] : 0.;
+      }
   return MCV_OK;
 }
 

@@ -55,4 +55,32 @@ int ic_harmonics_device(const IcArgs &a, cudaStream_t s);
 int ic_sums_device(const IcArgs &a, int mode, const double *x, double4 *partial, int blocks, cudaStream_t s);
 int ic_fields_device(const IcArgs &a, cudaStream_t s);
 
+// History-output staging (mcv_get_history): convert_wind_P2SP over the whole
+// padded array of one member (src/spatial_operators_mod.F90:391-405) after
+// addFillValue (src/output_mod.F90:230-248), with A IG evaluated per point from
+// the equiangular formulas.  Writes component `which` (0 zonal, 1 meridional)
+// in the caller's dense layout [6][npx][npx].  u, v: the member's pitched
+// fields [6][npx][P].
+int history_p2sp_device(const GeomArgs &a, const double *u, const double *v, int which, double *out,
+                        cudaStream_t s);
+
+// calc_VIA (src/diag_mod.F90:69-93) of a member's pitched field [6][npx][P]:
+// cell averages with the reference's weightsOnPV (mesh_mod.F90:183-203,
+// MCV4's /80 included), summed in its jDOF, iDOF order without FMA
+// contraction, into (ics:ice, jcs:jce, 6) = [6][nc+2][nc+2] with zero halo
+// cells (the layout of stat%uC).
+int via_device(int order, int nc, int npx, int P, const double *f, double *out, cudaStream_t s);
+
+// The normalized L1 / L2 / Linf of doc/orderCheck.m:63-81 between the cell
+// averages (calc_VIA) of two members' pitched fields a and b of one grid,
+// weighted by areaCell ([nc][nc], the same on every panel): per block
+// partial[2 b] = {sum |a-b| w, sum |b| w, sum (a-b)^2 w, sum b^2 w} and
+// partial[2 b + 1] = {max |a-b| w, max |b| w, 0, 0} over `blocks` blocks.
+int norms_device(int order, int nc, int npx, int P, const double *a, const double *b, const double *area,
+                 double4 *partial, int blocks, cudaStream_t s);
+
+// areaCell of one panel (src/mesh_mod.F90:205-212 with EquiangularAllAreas,
+// :240-276): [nc][nc] spherical-excess areas times radius^2.
+void equiangular_cell_areas(int nc, double radius, double *area);
+
 }  // namespace mcv

@@ -17,6 +17,7 @@
 // call's contents.  Each call overwrites every slot it later reads, so nothing
 // has to start at zero; two calls that overlap on the GPU (different host
 // threads or streams at the same time) race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -128,28 +129,71 @@ __global__ void noalloc_final_kernel(int members, double *scratch) {
   res[1] = es.s + es.c;
 }
 
-// Device address of the scratch array for the current device, looked up once
-// per device with that device current (the array's name in host code is only a
-// stand-in for it and must never reach a kernel).
+// Device address of the scratch array for the current device and context,
+// looked up with that device current (the array's name in host code is only a
+// stand-in for it and must never reach a kernel).  The address belongs to the
+// module loaded into one context: after cudaDeviceReset (or anything else that
+// destroys and recreates the device's primary context) the module is loaded
+// again, possibly elsewhere.  So the cache is keyed on the context's unique id
+// (cuCtxGetId: unique over the process's lifetime, unlike the CUcontext
+// handle, which a recreated primary context may reuse) and the address is
+// looked up again when the current context's id has changed.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+void *driver_fn(const char *name) {
+  void *p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+// id of the calling thread's current context; 0 if there is none yet
+bool current_ctx_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_ctx = (CtxGetCurrentFn)driver_fn("cuCtxGetCurrent");
+  static CtxGetIdFn get_id = (CtxGetIdFn)driver_fn("cuCtxGetId");
+  *id = 0;
+  if (!get_ctx || !get_id) return false;
+  CUcontext ctx = nullptr;
+  if (get_ctx(&ctx) != CUDA_SUCCESS) return false;
+  if (!ctx) return true;
+  return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+struct ScratchAddr {
+  unsigned long long ctx_id;
+  double *ptr;
+};
 std::mutex g_noalloc_mutex;
-double *g_noalloc_ptr[kNoallocMaxDevices] = {};
+ScratchAddr g_noalloc_addr[kNoallocMaxDevices] = {};
 
 int noalloc_scratch(double **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(MCV_ERR_CUDA, "mcv_mass_energy_noalloc: no current CUDA device");
   if (dev < 0 || dev >= kNoallocMaxDevices) return fail(MCV_ERR_CUDA, "mcv_mass_energy_noalloc: device index too large");
+  // id 0 before the runtime has bound a context to this thread; the symbol
+  // lookup below binds the device's primary context
+  unsigned long long id = 0;
+  if (!current_ctx_id(&id)) return fail(MCV_ERR_CUDA, "mcv_mass_energy_noalloc: cannot read the current CUDA context");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
+  ScratchAddr &a = g_noalloc_addr[dev];
+  if (id == 0 || !a.ptr || a.ctx_id != id) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
       cudaGetLastError();
       return fail(MCV_ERR_CUDA, "mcv_mass_energy_noalloc: cannot resolve the scratch array's device address");
     }
-    g_noalloc_ptr[dev] = (double *)p;
+    if (!current_ctx_id(&id) || id == 0)
+      return fail(MCV_ERR_CUDA, "mcv_mass_energy_noalloc: cannot read the current CUDA context");
+    a.ctx_id = id;
+    a.ptr = (double *)p;
   }
-  *out = g_noalloc_ptr[dev];
+  *out = a.ptr;
   return MCV_OK;
 }
 

@@ -46,6 +46,7 @@ struct Finished {
   std::vector<double> u, v, phi, phiG;
   long long nsteps;
   int finite;
+  int status = MCV_OK;  // < 0: the forecast failed (admission or read-back); no state
 };
 
 struct Pool {
@@ -117,12 +118,21 @@ void close_pool(Pool *p) {
   delete p;
 }
 
-// A pool of `slots` member slots on the grid (order, nc, dt), or nullptr with
-// *rc = MCV_OK when the budget has no room even after evicting idle empty pools.
+// A pool on the grid (order, nc, dt), or nullptr with *rc = MCV_OK when the
+// budget has no room for even one slot after evicting idle empty pools.  The
+// pool gets slots_for() slots, fewer where the budget left by the pools that
+// cannot be evicted (running, or holding a request) does not hold them: a
+// request waits only while those pools leave no room for one slot, never for
+// a pool larger than the budget (submit checked that one slot fits in it).
 Pool *new_pool(mcv_server *s, int order, int nc, double dt, int *rc) {
   *rc = MCV_OK;
-  const int slots = slots_for(s, order, nc);
+  long long pinned = 0;  // bytes of the pools that stay
+  for (const Pool *q : s->pools)
+    if (q->in_flight || !q->empty()) pinned += q->bytes;
+  int slots = slots_for(s, order, nc);
+  while (slots > 1 && pinned + footprint(s, order, nc, slots) > s->budget) --slots;
   const long long need = footprint(s, order, nc, slots);
+  if (pinned + need > s->budget) return nullptr;
   while (used_bytes(s) + need > s->budget) {
     // evict an idle, empty pool (the largest first)
     Pool *victim = nullptr;
@@ -208,7 +218,21 @@ long long chunk_steps(const mcv_server *s, const Pool *p) {
   return std::max(1LL, std::min(left, (long long)(s->chunk_ms / est)));
 }
 
-// The pool's chunk has ended: retire the forecasts it completed.
+// Record request `id` as failed with status rc (its result call reports rc).
+void fail_request(mcv_server *s, long long id, long long nsteps, int rc) {
+  Finished f;
+  f.nsteps = nsteps;
+  f.finite = 0;
+  f.status = rc;
+  s->finished[id] = std::move(f);
+  s->unreported.push_back(id);
+}
+
+// The pool's chunk has ended: retire the forecasts it completed.  The step
+// accounting and the slot lists are brought up to date before any call that
+// can fail; a forecast whose check or read-back fails is retired as failed
+// (its result call returns the error), so one bad forecast cannot wedge the
+// loop.  Returns the first error seen.
 int finish_chunk(mcv_server *s, Pool *p) {
   const long long steps = p->in_flight;
   p->in_flight = 0;
@@ -218,31 +242,39 @@ int finish_chunk(mcv_server *s, Pool *p) {
   std::vector<int> done, still;
   for (int slot : p->active) {
     p->left[slot] -= steps;
-    (p->left[slot] == 0 ? done : still).push_back(slot);
+    (p->left[slot] <= 0 ? done : still).push_back(slot);
   }
+  p->active = still;
   if (done.empty()) return MCV_OK;
   std::vector<int> flags(p->slots, 0);
-  const int frc = mcv_check_finite(p->h, flags.data());
-  if (frc != MCV_OK && frc != MCV_ERR_NONFINITE) return frc;
+  int first = mcv_check_finite(p->h, flags.data());
+  if (first == MCV_ERR_NONFINITE) first = MCV_OK;  // flagged per forecast below
   int npx, n, halo;
   mcv_grid_sizes(p->order, p->nc, &npx, &n, &halo);
   const size_t sz = (size_t)npx * npx * 6;
   for (int slot : done) {
+    const long long id = p->req[slot];
+    p->req[slot] = -1;
+    int rc = first;
     Finished f;
-    f.u.resize(sz);
-    f.v.resize(sz);
-    f.phi.resize(sz);
-    f.phiG.resize(sz);
-    if (int rc = mcv_get_state(p->h, slot, f.u.data(), f.v.data(), f.phi.data(), f.phiG.data())) return rc;
+    if (!rc) {
+      f.u.resize(sz);
+      f.v.resize(sz);
+      f.phi.resize(sz);
+      f.phiG.resize(sz);
+      rc = mcv_get_state(p->h, slot, f.u.data(), f.v.data(), f.phi.data(), f.phiG.data());
+    }
+    if (rc) {
+      fail_request(s, id, p->total[slot], rc);
+      if (!first) first = rc;
+      continue;
+    }
     f.nsteps = p->total[slot];
     f.finite = flags[slot] ? 0 : 1;
-    const long long id = p->req[slot];
     s->finished[id] = std::move(f);
     s->unreported.push_back(id);
-    p->req[slot] = -1;
   }
-  p->active = still;
-  return MCV_OK;
+  return first;
 }
 
 int check_grid(int order, int nc, double dt, long long nsteps) {
@@ -362,39 +394,71 @@ extern "C" int mcv_server_prepare(mcv_server *s, int order, int nc, double dt) {
 extern "C" int mcv_server_poll(mcv_server *s, long long *ids, int max_ids, int *n_ids) {
   if (!s || !n_ids || max_ids < 0 || (max_ids > 0 && !ids)) return fail(MCV_ERR_ARG, "bad poll arguments");
   *n_ids = 0;
-  // 1. chunks that ended
+  // 1. chunks that ended (a failed query or read-back retires the pool's
+  // finished forecasts as failed; the poll goes on and reports the error)
+  int chunk_err = MCV_OK;
   for (Pool *p : s->pools) {
     if (!p->in_flight) continue;
     const int q = mcv_query(p->h);
     if (q == MCV_BUSY) continue;
-    if (q != MCV_OK) return q;
-    if (int rc = finish_chunk(s, p)) return rc;
+    const int rc = (q != MCV_OK) ? q : finish_chunk(s, p);
+    if (q != MCV_OK) {
+      // the chunk's work is lost: its forecasts fail and their slots free up
+      p->in_flight = 0;
+      for (int slot : p->active) {
+        fail_request(s, p->req[slot], p->total[slot], q);
+        p->req[slot] = -1;
+      }
+      p->active.clear();
+    }
+    if (rc && !chunk_err) chunk_err = rc;
   }
   // 2. admission, first come first served among the requests that fit
+  // (a request whose initial state cannot be loaded is retired as failed and
+  // its error returned once; the others stay queued)
+  int first = MCV_OK;
   for (auto it = s->waiting.begin(); it != s->waiting.end();) {
     int placed;
-    if (int rc = admit(s, *it, &placed)) return rc;
+    if (int rc = admit(s, *it, &placed)) {
+      fail_request(s, it->id, it->nsteps, rc);
+      if (!first) first = rc;
+      it = s->waiting.erase(it);
+      continue;
+    }
     it = placed ? s->waiting.erase(it) : std::next(it);
   }
   // 3. the next chunk of every idle pool with active slots
   for (Pool *p : s->pools) {
     if (p->in_flight || p->active.empty()) continue;
+    int rc = MCV_OK;
     if (!p->dev_active_set || p->dev_active != p->active) {
-      if (int rc = mcv_set_active(p->h, (int)p->active.size(), p->active.data())) return rc;
-      p->dev_active = p->active;
-      p->dev_active_set = true;
+      rc = mcv_set_active(p->h, (int)p->active.size(), p->active.data());
+      if (!rc) {
+        p->dev_active = p->active;
+        p->dev_active_set = true;
+      }
     }
     const long long k = chunk_steps(s, p);
     p->launched = now_ms();
-    if (int rc = mcv_step_async(p->h, (int)k)) return rc;
+    if (!rc) rc = mcv_step_async(p->h, (int)k);
+    if (rc) {
+      // the pool cannot step: its forecasts fail and their slots free up
+      for (int slot : p->active) {
+        fail_request(s, p->req[slot], p->total[slot], rc);
+        p->req[slot] = -1;
+      }
+      p->active.clear();
+      if (!first) first = rc;
+      continue;
+    }
     p->in_flight = k;
   }
-  // 4. the forecasts finished since the last poll
+  // 4. the forecasts finished (or failed) since the last poll
   while (*n_ids < max_ids && !s->unreported.empty()) {
     ids[(*n_ids)++] = s->unreported.front();
     s->unreported.pop_front();
   }
-  return MCV_OK;
+  return chunk_err ? chunk_err : first;
 }
 
 extern "C" int mcv_server_result(mcv_server *s, long long id, double *u, double *v, double *phi, double *phiG,
@@ -412,6 +476,18 @@ extern "C" int mcv_server_result(mcv_server *s, long long id, double *u, double 
     return fail(MCV_ERR_ARG, "no such request (unknown, or its result was already taken)");
   }
   const Finished &f = it->second;
+  if (f.status != MCV_OK) {
+    const int st = f.status;
+    if (nsteps) *nsteps = f.nsteps;
+    if (finite) *finite = 0;
+    s->finished.erase(it);
+    for (auto q = s->unreported.begin(); q != s->unreported.end(); ++q)
+      if (*q == id) {
+        s->unreported.erase(q);
+        break;
+      }
+    return fail(st, "the forecast failed (its initial state, a step or its read-back returned this error)");
+  }
   const size_t bytes = f.u.size() * sizeof(double);
   if (u) std::memcpy(u, f.u.data(), bytes);
   if (v) std::memcpy(v, f.v.data(), bytes);

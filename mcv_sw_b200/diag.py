@@ -1,31 +1,44 @@
 """Host-side diagnostics on downloaded states.
 
-cell_average restates calc_VIA (src/diag_mod.F90:69-93): the weightsOnPV
-quadrature of a cell's DOF x DOF points (mesh_mod.F90:183-203).  The norms are
-the area-weighted L1/L2/Linf of doc/orderCheck.m:63-81 on cell averages.
+cell_average restates calc_VIA (src/diag_mod.F90:69-93) with the reference's
+weightsOnPV (src/mesh_mod.F90:183-203): the outer product of {1, 4, 1}/36
+(MCV3) or {1, 3, 3, 1}/80 (MCV4; its weights sum to 0.8, so its cell
+"averages" are 0.8 times the mean, as the reference's are), summed in the
+jDOF, iDOF order.  The norms are the areaCell-weighted L1/L2/Linf of
+doc/orderCheck.m:63-81 on those cell values; they are relative, so the 0.8
+cancels.  The device computes the same (Stepper.get_history,
+Stepper.height_error_norms) without downloading the state.
 """
 import numpy as np
 
+from . import api
+
+
+def pv_weights(order):
+    """weightsOnPV(iDOF, jDOF) as a (jDOF, iDOF) array."""
+    a = np.array([1.0, 4.0, 1.0]) if order == 3 else np.array([1.0, 3.0, 3.0, 1.0])
+    return np.outer(a, a) / (36.0 if order == 3 else 80.0)
+
 
 def cell_average(geom, field):
-    """(6, nc, nc) cell averages of a padded field (6, npx, npx)."""
+    """(6, nc, nc) calc_VIA values of a padded field (6, npx, npx)."""
     D, nc, H = geom.order, geom.nc, geom.H
-    w1 = np.array([1.0, 4.0, 1.0]) / 6.0 if D == 3 else np.array([1.0, 3.0, 3.0, 1.0]) / 8.0
+    w = pv_weights(D)
     out = np.zeros((6, nc, nc))
     for jd in range(D):
         for id_ in range(D):
-            out += (w1[jd] * w1[id_]) * field[:, H + jd: H + jd + (D - 1) * nc: D - 1,
-                                              H + id_: H + id_ + (D - 1) * nc: D - 1]
+            out = out + w[jd, id_] * field[:, H + jd: H + jd + (D - 1) * nc: D - 1,
+                                           H + id_: H + id_ + (D - 1) * nc: D - 1]
     return out
 
 
 def cell_areas(geom):
-    """Cell areas from the sqrtG quadrature (the same weights as the averages)."""
-    return cell_average(geom, geom.sqrtG)
+    """mesh%areaCell of the inner cells, (6, nc, nc)."""
+    return api.cell_areas(geom.nc, geom.radius)[:, 1:-1, 1:-1]
 
 
 def norms(geom, model, ref):
-    """Normalized (L1, L2, Linf) of model - ref on cell averages (orderCheck.m:63-81)."""
+    """Normalized (L1, L2, Linf) of model - ref on calc_VIA values (orderCheck.m:63-81)."""
     a, b, w = cell_average(geom, model), cell_average(geom, ref), cell_areas(geom)
     l1 = np.sum(np.abs(a - b) * w) / np.sum(np.abs(b) * w)
     l2 = np.sqrt(np.sum((a - b) ** 2 * w) / np.sum(b ** 2 * w))

@@ -184,8 +184,16 @@ class ForecastServer:
 
     # ---- pools ----
     def _new_pool(self, key):
+        """A pool of slots_for(key) slots, fewer where the budget left by the
+        pools that cannot be evicted (running, or holding a request) does not
+        hold them; None while those pools leave no room for one slot."""
+        pinned = sum(p.bytes for p in self.pools if p.in_flight or any(r is not None for r in p.req))
         slots = self.slots_for(key)
+        while slots > 1 and pinned + self.footprint(key, slots) > self.budget:
+            slots -= 1
         need = self.footprint(key, slots)
+        if pinned + need > self.budget:
+            return None
         while self.used + need > self.budget:
             # evict an idle, empty pool (the least useful memory first: largest)
             empty = [p for p in self.pools if not p.in_flight and all(r is None for r in p.req)]

@@ -1022,6 +1022,8 @@ void orc_sizes(const orc_ctx *c, int *out) {
   out[0] = c->nPVx; out[1] = c->nPVHalo; out[2] = (int)c->npx; out[3] = c->Nx; out[4] = (int)c->ncx;
 }
 double orc_dx(const orc_ctx *c) { return c->dx; }
+/* the time step (namelist dt, parameters_mod.F90:116) of an existing instance */
+void orc_set_dt(orc_ctx *c, double dt) { c->dt = dt; }
 
 /* Copy a mesh array out.  which: 0 xP,1 yP,2 lonP,3 latP,4 sqrtG,5 f,6 phi_s,
    7 matrixG,8 matrixIG,9 matrixA,10 matrixIA (4*NP), 11 areaCell (cells), 12 ghost coef (n*H),
@@ -1124,6 +1126,36 @@ void orc_linear_interp(orc_ctx *c, double *dest, const double *src, int h) { lin
 double orc_total_mass(const orc_ctx *c) { return calc_total_mass(c, &c->stat[c->old_slot]); }
 double orc_total_energy(const orc_ctx *c) { return calc_total_energy(c, &c->stat[c->old_slot]); }
 void orc_calc_VIA(const orc_ctx *c, double *out, const double *field) { calc_VIA(c, out, field); }
+
+/* output_mod.F90:230-248: FillValue in the four halo corner squares of u and v */
+static void addFillValue(orc_ctx *c, orc_stat *s) {
+  for (int p = 1; p <= 6; p++)
+    for (int j = c->jps; j <= c->jpe; j++)
+      for (int i = c->ips; i <= c->ipe; i++) {
+        int xc = i < c->ids || i > c->ide, yc = j < c->jds || j > c->jde;
+        if (xc && yc) {
+          s->u[PIX(c, i, j, p)] = FILLVALUE;
+          s->v[PIX(c, i, j, p)] = FILLVALUE;
+        }
+      }
+}
+
+/* MCV_SW.F90:62-67 on stat(old): addFillValue, convert_wind_P2SP, then calc_VIA
+   of u, v, phi; copies out u, v, phi, zonal, meridional (padded) and uC, vC,
+   phiC ((ics:ice, jcs:jce, 6), halo cells 0).  Any output may be NULL. */
+void orc_history(orc_ctx *c, double *u, double *v, double *phi, double *zonal, double *merid, double *uC, double *vC,
+                 double *phiC) {
+  orc_stat *s = &c->stat[c->old_slot];
+  addFillValue(c, s);
+  convert_wind_P2SP(c, s);
+  if (uC) calc_VIA(c, uC, s->u);
+  if (vC) calc_VIA(c, vC, s->v);
+  if (phiC) calc_VIA(c, phiC, s->phi);
+  double *dst[5] = {u, v, phi, zonal, merid};
+  const double *src[5] = {s->u, s->v, s->phi, s->zonal_wind, s->meridional_wind};
+  for (int k = 0; k < 5; k++)
+    if (dst[k]) memcpy(dst[k], src[k], c->NP * 8);
+}
 
 int orc_num_threads(void) {
 #ifdef _OPENMP

@@ -60,6 +60,16 @@ def _load():
     lib.orc_total_energy.restype = ctypes.c_double
     lib.orc_total_energy.argtypes = [ctypes.c_void_p]
     lib.orc_calc_VIA.argtypes = [ctypes.c_void_p, _D, _D]
+    lib.orc_set_dt.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.orc_history.argtypes = [ctypes.c_void_p] + [_D] * 8
+    _L = ctypes.c_long
+    lib.orc_ic_tilted_zonal.argtypes = [_L, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, _D, _D, _D]
+    lib.orc_ic_add_harmonics.restype = ctypes.c_int
+    lib.orc_ic_add_harmonics.argtypes = [_L, _D, _D, ctypes.c_int, _D, ctypes.c_double, _D]
+    lib.orc_ic_add_mountain.argtypes = [_L, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, _D, _D]
+    lib.orc_ic_add_rossby_wave.argtypes = [_L, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_double, _D, _D, _D]
     lib.orc_num_threads.restype = ctypes.c_int
     lib.orc_set_num_threads.argtypes = [ctypes.c_int]
     _lib = lib
@@ -147,6 +157,10 @@ class Oracle:
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v, phi)]
         self.lib.orc_set_state_cov(self.h, *[_dp(x) for x in a])
 
+    def set_dt(self, dt):
+        self.dt = float(dt)
+        self.lib.orc_set_dt(self.h, self.dt)
+
     def step(self, nsteps=1):
         self.lib.orc_step(self.h, int(nsteps))
 
@@ -194,6 +208,19 @@ class Oracle:
     def calc_VIA(self, field):
         out = np.empty((6, self.ncx, self.ncx))
         self.lib.orc_calc_VIA(self.h, _dp(out), _dp(np.ascontiguousarray(field, dtype=np.float64)))
+        return out
+
+
+    def history(self):
+        """The history-output sequence of the reference's time loop
+        (MCV_SW.F90:62-67) on the current state: addFillValue, convert_wind_P2SP,
+        calc_VIA of u, v, phi.  Returns a dict of padded fields u, v, phi,
+        zonal, merid and cell fields uC, vC, phiC of shape (6, Nc+2, Nc+2)
+        (halo cells 0)."""
+        out = {k: np.empty(self.pshape) for k in ("u", "v", "phi", "zonal", "merid")}
+        out.update({k: np.empty((6, self.ncx, self.ncx)) for k in ("uC", "vC", "phiC")})
+        self.lib.orc_history(self.h, *[_dp(out[k]) for k in ("u", "v", "phi", "zonal", "merid", "uC", "vC",
+                                                             "phiC")])
         return out
 
 

@@ -2,7 +2,9 @@
 // libmcv_gpu.so, so that mcv_server.cpp (compiled unchanged) runs on a CPU.
 // A fake member's "state" records the seed it was loaded with and the steps
 // it was advanced: a forecast stepped too far or too little shows up exactly.
-// A queued chunk completes after two mcv_query calls.
+// A queued chunk completes after two mcv_query calls.  Two injected failures
+// exercise the loop's error paths: a balanced-flow spec with gh0 < 0 is
+// refused, and a member loaded with the seed 666 fails its read-back.
 #include <cstring>
 #include <string>
 #include <vector>
@@ -83,6 +85,7 @@ int mcv_set_member(mcv_handle *h, int m, const double *phi_s, const double *, co
 int mcv_set_member_balanced_flow(mcv_handle *h, int m, double gh0, double, double, int, const double *, double, double,
                                  double, double, double) {
   if (!h->geometry || h->pending) return mcv::fail(MCV_ERR_ORDER, "member set on a busy handle or before geometry");
+  if (gh0 < 0.) return mcv::fail(MCV_ERR_ARG, "injected: a spec this fake refuses");
   h->seed[m] = gh0;
   h->steps[m] = 0;
   return MCV_OK;
@@ -128,6 +131,7 @@ int mcv_check_finite(mcv_handle *h, int *flags) {
 
 int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double *phi, double *phiG) {
   if (h->pending) return mcv::fail(MCV_ERR_ORDER, "download from a busy handle");
+  if (h->seed[m] == 666.) return mcv::fail(MCV_ERR_CUDA, "injected: a read-back this fake fails");
   const size_t sz = (size_t)h->npx * h->npx * 6;
   for (size_t k = 0; k < sz; ++k) {
     if (u) u[k] = h->seed[m];

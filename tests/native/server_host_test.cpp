@@ -136,6 +136,70 @@ int main() {
     CHECK(mcv_server_submit(s, 4, 4, 60., 2, f.data(), f.data(), f.data(), f.data(), &id) == MCV_ERR_NOMEM);
     CHECK(mcv_server_destroy(s) == MCV_OK);
   }
+  {
+    // slot_bytes allows 32 slots but the budget holds one member: the pool is
+    // made with the slots the budget holds, and every request is served
+    // (2200 bytes for one member of (3, 4) with the fake footprint, 3400 for two)
+    mcv_server *s = nullptr;
+    CHECK(mcv_server_create(MCV_FP64, MCV_RK4, 6.371e6, 2500, 1LL << 30, 32, 0.1, -1, &s) == MCV_OK);
+    std::map<long long, Expect> want;
+    for (int i = 0; i < 3; ++i) CHECK(submit_host(s, 3, 4, 60., 2 + i, 20. + i, want) == 0);
+    CHECK(drain(s, want, st) == 0);
+    CHECK(st[6] == 1 && st[5] == 2200);  // one pool of one slot
+    CHECK(mcv_server_destroy(s) == MCV_OK);
+    CHECK(g_live_handles == 0);
+  }
+  {
+    // a request whose initial state is refused and one whose read-back fails
+    // are retired as failed (their result calls return the error, once); the
+    // poll reports each error and the other forecasts still finish
+    mcv_server *s = nullptr;
+    CHECK(mcv_server_create(MCV_MIXED, MCV_RK3_TVD, 6.371e6, 1LL << 40, 2400, 32, 0.1, -1, &s) == MCV_OK);
+    std::map<long long, Expect> want;
+    long long bad_spec = 0, bad_read = 0;
+    CHECK(mcv_server_submit_balanced_flow(s, 3, 4, 100., 5, -1., 0., 0., 0, nullptr, 0., 0., 0., 0., 0., &bad_spec) ==
+          MCV_OK);
+    {
+      const int npx = npx_of(3, 4);
+      std::vector<double> f((size_t)npx * npx * 6, 666.);
+      CHECK(mcv_server_submit(s, 3, 4, 100., 3, f.data(), f.data(), f.data(), f.data(), &bad_read) == MCV_OK);
+    }
+    for (int i = 0; i < 4; ++i) CHECK(submit_host(s, 3, 4, 100., 4 + i, 30. + i, want) == 0);
+    int errors = 0;
+    bool got_spec = false, got_read = false;
+    for (int iter = 0; iter < 200000 && (!want.empty() || !got_spec || !got_read); ++iter) {
+      long long ids[4];
+      int n = 0;
+      const int rc = mcv_server_poll(s, ids, 4, &n);
+      if (rc != MCV_OK) ++errors;
+      for (int k = 0; k < n; ++k) {
+        if (ids[k] == bad_spec || ids[k] == bad_read) {
+          long long steps = -1;
+          int finite = -1;
+          const int want_rc = ids[k] == bad_spec ? MCV_ERR_ARG : MCV_ERR_CUDA;
+          CHECK(mcv_server_result(s, ids[k], nullptr, nullptr, nullptr, nullptr, &steps, &finite) == want_rc);
+          CHECK(finite == 0 && steps == (ids[k] == bad_spec ? 5 : 3));
+          CHECK(mcv_server_result(s, ids[k], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr) == MCV_ERR_ARG);
+          (ids[k] == bad_spec ? got_spec : got_read) = true;
+          continue;
+        }
+        auto it = want.find(ids[k]);
+        CHECK(it != want.end());
+        const size_t sz = (size_t)it->second.npx * it->second.npx * 6;
+        std::vector<double> u(sz), v(sz);
+        long long steps = -1;
+        int finite = -1;
+        CHECK(mcv_server_result(s, ids[k], u.data(), v.data(), nullptr, nullptr, &steps, &finite) == MCV_OK);
+        CHECK(u[0] == it->second.seed && v[0] == (double)it->second.nsteps && finite == 1);
+        want.erase(it);
+      }
+    }
+    CHECK(want.empty() && got_spec && got_read && errors == 2);
+    CHECK(mcv_server_stats(s, st) == MCV_OK);
+    CHECK(st[0] == 0 && st[1] == 0 && st[2] == 0);
+    CHECK(mcv_server_destroy(s) == MCV_OK);
+    CHECK(g_live_handles == 0);
+  }
   std::printf("ok\n");
   return 0;
 }

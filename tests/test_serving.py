@@ -135,6 +135,19 @@ def test_admission_waits_for_budget_and_evicts_idle_pools():
     assert FakeStepper.created[0].closed
 
 
+def test_pool_sized_to_the_budget_when_slot_bytes_allow_more():
+    # slot_bytes would give max_slots slots, the budget holds one member: the
+    # pool is made with one slot and the requests are served one at a time
+    FakeStepper.created = []
+    reqs = requests([(0.0, 3, 8, 1.0 + k) for k in range(3)])
+    srv = serving.ForecastServer(stepper_factory=FakeStepper, footprint_fn=fake_footprint, keep_states=True,
+                                 poll_s=0.0, slot_bytes=10 ** 12, chunk_ms=1e-3,
+                                 hbm_budget=fake_footprint(3, 8, None, None, 1))
+    res = srv.run(reqs)
+    assert all(r.state["steps"] == r.nsteps for r in res)
+    assert srv.stats["pools_created"] == 1 and FakeStepper.created[0].members == 1
+
+
 def test_summary():
     reqs = requests([(0.0, 3, 8, 2.0), (0.0, 3, 8, 4.0)])
     s = serving.summarize(server().run(reqs))
