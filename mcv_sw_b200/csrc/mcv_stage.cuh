@@ -402,7 +402,7 @@ struct Tile {
   // cV, sqrtG f) ...
   static constexpr int SG = (PAIRED ? 10 : 6) * A, CU = SG + I, CV = CU + I, FC = CV + I;
   // ... interface eigenvalues and upwind signs ...
-  static constexpr int LAMX = FC + I;                // [TY][CX+1]
+  static constexpr int LAMX = CV + (PAIRED ? 2 : 1) * I;  // [TY][CX+1]
   static constexpr int SGNX = LAMX + TY * (CX + 1);
   static constexpr int LAMY = SGNX + TY * (CX + 1);  // [TX][CY+1]
   static constexpr int SGNY = LAMY + TX * (CY + 1);
@@ -516,6 +516,11 @@ __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddep
 
 // MINB: CTAs per SM the register allocation must allow (launch bounds).
 // WALK: 0 -- sweeps as per-cell items; n -- sweeps as walks of n cells.
+// OPT bit 1 (split precision with walks): balanced sweeps -- the one-quantity
+// walks are twice as long as the packed-pair walks, so that items cost alike
+// (all stages but the last, whose longer walks would spill registers).
+// OPT bit 2 (TMA form, rows of 28..32 points): each thread forms its loaded
+// column's linear references once per work item instead of once per point.
 // TMA: persistent form -- each CTA walks work items (tile, panel, member)
 // blockIdx.x, blockIdx.x + gridDim.x, ...; the next item's input fields are
 // copied into a shared-memory staging area by TMA while the current item's
@@ -524,7 +529,7 @@ __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddep
 // linear references in the step's first stage and stores them, and the later
 // stages' copies bring them in with the tile.  Otherwise one CTA per (tile,
 // panel, member) loads its fields with ordinary loads.
-template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA>
+template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA, int OPT>
 __global__ void __launch_bounds__(NT, MINB)
     stage_kernel(const GridDesc g, const StageArgs a, const __grid_constant__ TileMaps tm) {
   using R = std::conditional_t<MIXED, float, double>;
@@ -745,11 +750,25 @@ __global__ void __launch_bounds__(NT, MINB)
     }
   };
 
+  // the linear references on column X (split precision; unused in FP64)
+  auto column_refs = [&](double X, double *pref) {
+    if constexpr (MIXED) {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        pref[q] = __fma_rn(plane[3 * q + 1], X, plane[3 * q]);
+        pref[3 + q] = plane[3 * q + 2];
+      }
+    }
+  };
+
   // one loaded point: r = {u, v, phi, phi_s, sqrtG, G^11, G^12, G^22} (FP64
   // policy) or {Y_u, Y_v, Y_phi} with f = {phi_s, d_u, d_v, d_phi} (split)
   // (X, Y) = (lx - H, ly - H) as doubles, the linear references' coordinates
-  auto point = [&](int idx, int lx, int ly, double X, double Y, const double *r, const float *f, const double4 &mx,
-                   const double4 &my) {
+  // pref: the linear references' values on the point's column, {E, u, v} at
+  // (X, 0) (pref[0..2]) and their slopes per point index in y (pref[3..5]):
+  // the reference at (X, Y) is fma(pref[3+q], Y, pref[q])
+  auto point = [&](int idx, int lx, int ly, double Y, const double *pref, const double *r, const float *f,
+                   const double4 &mx, const double4 &my) {
     // interior points also keep sqrtG, cU, cV (and f) and form the interface
     // eigenvalues and upwind signs; split precision rounds those to FP32 here
     auto interior = [&](R sg, R cu, R cv, R fc, R g11, R g22, R phi) {
@@ -792,9 +811,9 @@ __global__ void __launch_bounds__(NT, MINB)
       }
       MixPoint mp;
       mix_point(mp, mx, my, u64, v64, p64, (double)f[0], phibar, panel, a.two_omega, a.r2);
-      const float e = (float)(mp.q[0] - (plane[0] + plane[1] * X + plane[2] * Y));
-      const float uu = (float)(mp.q[1] - (plane[3] + plane[4] * X + plane[5] * Y));
-      const float vv = (float)(mp.q[2] - (plane[6] + plane[7] * X + plane[8] * Y));
+      const float e = (float)(mp.q[0] - __fma_rn(pref[3], Y, pref[0]));
+      const float uu = (float)(mp.q[1] - __fma_rn(pref[4], Y, pref[1]));
+      const float vv = (float)(mp.q[2] - __fma_rn(pref[5], Y, pref[2]));
       // the mass fluxes as FP32 products of the rounded phiG and winds
       const float pg = (float)mp.q[3], cu = (float)mp.cu, cv = (float)mp.cv;
       float2 *s2 = reinterpret_cast<float2 *>(sm);
@@ -866,15 +885,17 @@ __global__ void __launch_bounds__(NT, MINB)
       if (lx < lxe) {
         const bool xh = (lx < H) || (lx >= lxe - H);
         const double4 mx = MIXED ? metx[lx] : double4{};
-        const double X = (double)(lx - H);
+        double pref[6];  // the column's linear references (OPT bit 2: once per item)
+        if constexpr ((OPT & 2) != 0) column_refs((double)(lx - H), pref);
         double Y = (double)((int)(threadIdx.x >> 5) - H);
         for (int ly = threadIdx.x >> 5; ly < lye; ly += NT / 32, Y += (double)(NT / 32)) {
           const bool yh = (ly < H) || (ly >= lye - H);
           if (xh && yh) continue;  // tile corners are never read
+          if constexpr ((OPT & 2) == 0) column_refs((double)(lx - H), pref);
           double r[8];
           float f[4];
           staged(lx, ly, r, f);
-          point(ly * LX + lx, lx, ly, X, Y, r, f, mx, MIXED ? mety[ly] : mx);
+          point(ly * LX + lx, lx, ly, Y, pref, r, f, mx, MIXED ? mety[ly] : mx);
         }
       }
     } else {
@@ -886,7 +907,9 @@ __global__ void __launch_bounds__(NT, MINB)
         float f[4];
         staged(lx, ly, r, f);
         const double4 zero{};
-        point(idx, lx, ly, (double)(lx - H), (double)(ly - H), r, f, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
+        double pref[6];
+        column_refs((double)(lx - H), pref);
+        point(idx, lx, ly, (double)(ly - H), pref, r, f, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
       }
     }
   } else {
@@ -948,8 +971,9 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
         for (int j = 0; j < 4; ++j) ff[j] = f[j][k];
         const double4 zero{};
-        point(idx, lx, ly, (double)(lx - H), (double)(ly - H), rr, ff, MIXED ? metx[lx] : zero,
-              MIXED ? mety[ly] : zero);
+        double pref[6];
+        column_refs((double)(lx - H), pref);
+        point(idx, lx, ly, (double)(ly - H), pref, rr, ff, MIXED ? metx[lx] : zero, MIXED ? mety[ly] : zero);
       }
     }
   }
@@ -963,7 +987,51 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   const Widths<R> w(g);
 
-  if constexpr (MIXED && WALK > 0) {
+  if constexpr (MIXED && WALK > 0 && (OPT & 1) && !last_stage(KIND)) {
+    // ---- phase W (split precision), balanced: kind 0 (the (E, phiG c^i)
+    // pair with Riemann on (wind component, phiG), packed FP32 pairs) walks
+    // segments of WALK cells, kind 1 (dvdx / dudy upwinded by sign(c^i), one
+    // quantity) segments of 2 WALK cells, so that every item costs about the
+    // same; items: x kind 0, y kind 0, x kind 1, y kind 1 (line fastest)
+    constexpr int S0X = WALK < CX ? WALK : CX, S0Y = WALK < CY ? WALK : CY;
+    constexpr int S1X = 2 * WALK < CX ? 2 * WALK : CX, S1Y = 2 * WALK < CY ? 2 * WALK : CY;
+    constexpr int N0X = (CX + S0X - 1) / S0X, N0Y = (CY + S0Y - 1) / S0Y;
+    constexpr int N1X = (CX + S1X - 1) / S1X, N1Y = (CY + S1Y - 1) / S1Y;
+    constexpr int E0X = T::TY * N0X, E0Y = E0X + T::TX * N0Y, E1X = E0Y + T::TY * N1X, E1Y = E1X + T::TX * N1Y;
+    const float2 *s2 = reinterpret_cast<const float2 *>(sm);
+    for (int it = threadIdx.x; it < E1Y; it += NT) {
+      if (it < E0X) {
+        const int r = it % T::TY, c0 = (it / T::TY) * S0X;
+        if (r >= tye || c0 >= ncx) continue;
+        const int w0 = (r + H) * LX + c0 * (D - 1);
+        R *xr = sm + T::XR + r * T::TX + c0 * (D - 1);
+        line_walk2<D, S0X, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, sm + T::LAMX + r * (CX + 1) + c0,
+                                 min(S0X, ncx - c0), c0 + S0X >= ncx, xr, xr + T::I, w);
+      } else if (it < E0Y) {
+        const int j = it - E0X, q = j % T::TX, c0 = (j / T::TX) * S0Y;
+        if (q >= txe || c0 >= ncy) continue;
+        const int w0 = c0 * (D - 1) * LX + (q + H);
+        R *yr = sm + T::YR + q + c0 * (D - 1) * T::TX;
+        line_walk2<D, S0Y, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, sm + T::LAMY + q * (CY + 1) + c0,
+                                      min(S0Y, ncy - c0), c0 + S0Y >= ncy, yr, yr + T::I, w);
+      } else if (it < E1X) {
+        const int j = it - E0Y, r = j % T::TY, c0 = (j / T::TY) * S1X;
+        if (r >= tye || c0 >= ncx) continue;
+        const int w0 = (r + H) * LX + c0 * (D - 1);
+        R *xr = sm + T::XR + 2 * T::I + r * T::TX + c0 * (D - 1);
+        line_walk<D, S1X, 1, 1, true, R>(sm + T::V + w0, sm + T::V + w0, sm + T::SGNX + r * (CX + 1) + c0,
+                                         min(S1X, ncx - c0), c0 + S1X >= ncx, xr, w);
+      } else {
+        const int j = it - E1X, q = j % T::TX, c0 = (j / T::TX) * S1Y;
+        if (q >= txe || c0 >= ncy) continue;
+        const int w0 = c0 * (D - 1) * LX + (q + H);
+        R *yr = sm + T::YR + 2 * T::I + q + c0 * (D - 1) * T::TX;
+        line_walk<D, S1Y, LX, T::TX, true, R>(sm + T::U + w0, sm + T::U + w0, sm + T::SGNY + q * (CY + 1) + c0,
+                                              min(S1Y, ncy - c0), c0 + S1Y >= ncy, yr, w);
+      }
+    }
+    __syncthreads();
+  } else if constexpr (MIXED && WALK > 0) {
     // ---- phase W (split precision): walks of WALK cells, item = (line,
     // segment, kind); kind 0: the (E, phiG c^i) pair with Riemann on (wind
     // component, phiG); kind 1: dvdx / dudy upwinded by sign(c^i)
@@ -1367,7 +1435,7 @@ struct StageLauncher {
   int (*blocks_per_sm)();   // resident CTAs per SM (sizes the persistent grid)
 };
 
-template <int D, int CX, int CY, int NT, int MINB, bool MIXED, int WALK, bool TMA = false>
+template <int D, int CX, int CY, int NT, int MINB, bool MIXED, int WALK, bool TMA = false, int OPT = 0>
 struct StageConfig {
   using T = Tile<D, CX, CY, std::conditional_t<MIXED, float, double>>;
   static constexpr size_t SMEM = TMA ? T::bytes_tma(MIXED) : T::bytes(MIXED);
@@ -1389,13 +1457,13 @@ struct StageConfig {
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA>, g, a, tm);
+    cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT>, g, a, tm);
   }
   template <int KIND>
   static cudaError_t attr() {
     // (the driver's own carveout choice: forcing the largest shared-memory
     // carveout shrank L1 and slowed the FP64 kernels by up to 20%)
-    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA>,
+    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
   static cudaError_t prepare() {
@@ -1407,7 +1475,7 @@ struct StageConfig {
   }
   static int blocks_per_sm() {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA>, NT,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT>, NT,
                                                       SMEM) != cudaSuccess)
       return 0;
     return n;

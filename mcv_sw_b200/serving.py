@@ -436,5 +436,6 @@ def summarize(results):
     makespan = max(r.finished for r in results) - min(r.arrival for r in results)
     return {"requests": len(results), "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
-            "sim_days": days, "makespan_s": makespan, "sim_days_per_s": days / makespan,
-            "all_finite": all(r.finite for r in results)}
+            "sim_days": float(days), "makespan_s": float(makespan), "sim_days_per_s": float(days / makespan),
+            "all_finite": all(r.finite for r in results),
+            "nonfinite_ids": [int(r.id) for r in results if not r.finite]}
