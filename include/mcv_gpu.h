@@ -150,6 +150,33 @@ int mcv_check_finite(mcv_handle *h, int *flags);
  * mcv_sync reports and return. */
 int mcv_selftest_wait(int complete, double limit_ms, int *timed_out, double *elapsed_ms);
 
+/* ---------------------------------------------------------------------
+ * Groups: several grids in one persistent launch.  No counterpart in the
+ * reference (one grid per process).  A group advances 1..4 handles of one
+ * order, precision, scheme and device -- any Nc, dt and member counts -- with
+ * one launch of the stage kernel per RK stage over the work items of all of
+ * them (each grid with its own geometry, dt and state buffers), followed by
+ * each grid's halo kernel; a group step is one CUDA graph.  tile: the
+ * stage-kernel candidate of the launch (mcv_tuning's index of a persistent
+ * TMA form), or -1 for the first handle's choice.  Each handle's result is
+ * bit for bit that of the handle stepped alone on the same candidate.  The
+ * handles keep working alone as well: the group orders its work after what
+ * is queued on their streams, and their later work after the group's.
+ * ------------------------------------------------------------------- */
+typedef struct mcv_group mcv_group;
+int mcv_group_create(mcv_handle *const *handles, int count, int tile, mcv_group **out);
+/* Queue nsteps RK steps of every handle's active members (handles with none
+ * are skipped); mcv_group_step also waits. */
+int mcv_group_step_async(mcv_group *g, int nsteps);
+int mcv_group_step(mcv_group *g, int nsteps);
+/* Wait for the group's queued steps; reports a stage kernel's error flag. */
+int mcv_group_sync(mcv_group *g);
+/* MCV_OK if the group's queued steps have finished, MCV_BUSY otherwise. */
+int mcv_group_query(mcv_group *g);
+/* Advance nsteps and return their device time (CUDA events on the group's stream). */
+int mcv_group_time_steps(mcv_group *g, int nsteps, double *ms);
+int mcv_group_destroy(mcv_group *g);
+
 /* Download member m's state over the padded range (any pointer may be NULL).
  * phiG = phi * sqrtG as src/time_scheme_mod.F90:85 stores it. */
 int mcv_get_state(mcv_handle *h, int m, double *u, double *v, double *phi, double *phiG);

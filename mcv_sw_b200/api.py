@@ -70,6 +70,13 @@ def lib():
         "mcv_get_state": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D]),
         "mcv_mass_energy": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
         "mcv_get_history": (ctypes.c_int, [vp, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D]),
+        "mcv_group_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
+        "mcv_group_step_async": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mcv_group_step": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mcv_group_sync": (ctypes.c_int, [vp]),
+        "mcv_group_query": (ctypes.c_int, [vp]),
+        "mcv_group_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _D]),
+        "mcv_group_destroy": (ctypes.c_int, [vp]),
         "mcv_height_error_norms": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, _D]),
         "mcv_cell_areas": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
         "mcv_destroy": (ctypes.c_int, [vp]),
@@ -426,6 +433,58 @@ class Stepper:
         out = (ctypes.c_double * 3)()
         _check(lib().mcv_height_error_norms(self.h, int(m), ref.h, int(ref_m), out))
         return tuple(out)
+
+
+class Group:
+    """Several Steppers (one order, precision and scheme; any Nc, dt, members)
+    advanced together, one batched stage-kernel launch per RK stage
+    (mcv_group_*).  tile: the candidate index of the launch, or -1 for the
+    first stepper's choice."""
+
+    def __init__(self, steppers, tile=-1):
+        self.steppers = list(steppers)
+        arr = (ctypes.c_void_p * len(self.steppers))(*[s.h for s in self.steppers])
+        g = ctypes.c_void_p()
+        _check(lib().mcv_group_create(arr, len(self.steppers), int(tile), ctypes.byref(g)))
+        self.g = g
+
+    def step(self, nsteps):
+        _check(lib().mcv_group_step(self.g, int(nsteps)))
+
+    def step_async(self, nsteps):
+        _check(lib().mcv_group_step_async(self.g, int(nsteps)))
+
+    def sync(self):
+        _check(lib().mcv_group_sync(self.g))
+
+    def query(self):
+        rc = lib().mcv_group_query(self.g)
+        if rc == BUSY:
+            return False
+        _check(rc)
+        return True
+
+    def time_steps(self, nsteps):
+        ms = ctypes.c_double()
+        _check(lib().mcv_group_time_steps(self.g, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "g", None):
+            lib().mcv_group_destroy(self.g)
+            self.g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 SERVER_STATS = ("waiting", "running", "unclaimed", "pools", "busy_pools", "pool_bytes", "pools_created",

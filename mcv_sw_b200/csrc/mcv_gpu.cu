@@ -363,20 +363,35 @@ HaloArgs halo_args(mcv_handle *h, int s, int c) {
   return a;
 }
 
-void launch_halo(mcv_handle *h, int s, int c) {
-  const HaloArgs a = halo_args(h, s, c);
-  const bool mixed_inc = h->mixed && !last_stage(stage_kind(h, s));
-  const long long threads = 24LL * (h->H + 1) * h->g.n * h->n_active;
+// The halo kernel of stage s over `count` handles (one order and arithmetic)
+// with buffer parities curs, one launch.
+template <int NB>
+void launch_halo_batch(mcv_handle *const *hs, const int *curs, int count, int s, cudaStream_t st) {
+  HaloBatch<NB> b;
+  std::memset(&b, 0, sizeof(b));
+  long long threads = 0;
+  for (int k = 0; k < count; ++k) {
+    mcv_handle *h = hs[k];
+    b.g[k] = h->g;
+    b.a[k] = halo_args(h, s, curs[k]);
+    b.first[k] = threads;
+    threads += 24LL * (h->H + 1) * h->g.n * h->n_active;
+  }
+  b.first[count] = threads;
+  b.ngrids = count;
+  const bool mixed_inc = hs[0]->mixed && !last_stage(stage_kind(hs[0], s));
   const int block = 128;
   const unsigned grid = (unsigned)((threads + block - 1) / block);
-  if (h->order == 3) {
-    if (mixed_inc) halo_kernel<3, true><<<grid, block, 0, h->stream>>>(h->g, a);
-    else halo_kernel<3, false><<<grid, block, 0, h->stream>>>(h->g, a);
+  if (hs[0]->order == 3) {
+    if (mixed_inc) halo_kernel<3, true, NB><<<grid, block, 0, st>>>(b);
+    else halo_kernel<3, false, NB><<<grid, block, 0, st>>>(b);
   } else {
-    if (mixed_inc) halo_kernel<4, true><<<grid, block, 0, h->stream>>>(h->g, a);
-    else halo_kernel<4, false><<<grid, block, 0, h->stream>>>(h->g, a);
+    if (mixed_inc) halo_kernel<4, true, NB><<<grid, block, 0, st>>>(b);
+    else halo_kernel<4, false, NB><<<grid, block, 0, st>>>(b);
   }
 }
+
+void launch_halo(mcv_handle *h, int s, int c) { launch_halo_batch<1>(&h, &c, 1, s, h->stream); }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
@@ -433,23 +448,56 @@ int stage_maps(mcv_handle *h, const StageLauncher &L, const StageArgs &a, int ki
   return MCV_OK;
 }
 
-int launch_stage(mcv_handle *h, int cand, int s, int c) {
-  const StageLauncher &L = h->cands[cand];
+// Grid k of a stage launch: the handle's grid descriptor with the candidate's
+// tiles, its stage arguments, tensor maps and work items (edge-free ones first).
+template <int NB>
+int add_grid(StageBatch<NB> &b, int k, mcv_handle *h, const StageLauncher &L, int s, int c) {
   GridDesc g = h->g;
   g.tiles_x = (h->nc + L.CX - 1) / L.CX;
   g.tiles_y = (h->nc + L.CY - 1) / L.CY;
-  const StageArgs a = stage_args(h, s, c);
-  const int kind = stage_kind(h, s);
-  TileMaps tm;
+  b.g[k] = g;
+  b.a[k] = stage_args(h, s, c);
+  b.slots[k] = h->n_active;
+  TileMaps &tm = b.tm[k];
   std::memset(&tm, 0, sizeof(tm));
   tm.total = g.tiles_x * g.tiles_y * 6 * h->n_active;  // work items (tile, panel, member)
+  if (L.tma)
+    if (int rc = stage_maps(h, L, b.a[k], stage_kind(h, s), tm)) return rc;
+  return MCV_OK;
+}
+
+// Item ranges of a batch of `n` grids: every grid's edge-free items, then
+// every grid's edge items.
+template <int NB>
+void number_items(StageBatch<NB> &b, int n) {
+  b.ngrids = n;
+  int nin = 0, ned = 0;
+  for (int k = 0; k < n; ++k) {
+    const int fin = edge_free_tiles(b.g[k].tiles_x, b.g[k].tiles_y) * 6 * b.slots[k];
+    b.in0[k] = nin;
+    b.ed0[k] = ned;
+    nin += fin;
+    ned += b.tm[k].total - fin;
+  }
+  b.in0[n] = nin;
+  b.ed0[n] = ned;
+  b.nin = nin;
+  b.total = nin + ned;
+}
+
+int launch_stage(mcv_handle *h, int cand, int s, int c) {
+  const StageLauncher &L = h->cands[cand];
+  StageBatch<1> b;
+  std::memset(&b, 0, sizeof(b));
+  if (int rc = add_grid(b, 0, h, L, s, c)) return rc;
+  number_items(b, 1);
+  const int kind = stage_kind(h, s);
   if (!L.tma) {
-    L.launch[kind](dim3(g.tiles_x * g.tiles_y, 6, h->n_active), h->stream, g, a, tm);
+    L.launch[kind](dim3(b.g[0].tiles_x * b.g[0].tiles_y, 6, h->n_active), h->stream, b);
     return MCV_OK;
   }
-  if (int rc = stage_maps(h, L, a, kind, tm)) return rc;
-  const int ctas = std::max(1, std::min(tm.total, h->bps[cand] * h->nsm));
-  L.launch[kind](dim3(ctas), h->stream, g, a, tm);
+  const int ctas = std::max(1, std::min(b.total, h->bps[cand] * h->nsm));
+  L.launch[kind](dim3(ctas), h->stream, b);
   return MCV_OK;
 }
 
@@ -1508,5 +1556,238 @@ extern "C" int mcv_select_tile(mcv_handle *h, int index) {
     }
   h->choice = index;  // -1: autotune again before the next step
   if (index >= 0 && (int)h->tune_ms.size() != h->ncands) h->tune_ms.assign(h->ncands, -1.f);
+  return MCV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Groups: several handles (grids of one order, arithmetic and scheme, any Nc,
+// dt and members) advanced together, each stage one batched launch of the
+// stage kernel over all of them followed by each grid's halo kernel.
+// ---------------------------------------------------------------------------
+struct mcv_group {
+  std::vector<mcv_handle *> hs;
+  int cand = -1;  // stage-kernel candidate every grid of the group uses
+  int bps = 0;    // resident CTAs per SM of the batched kernel
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  std::vector<cudaEvent_t> ready;  // per handle: work queued on its own stream before a group step
+  // step graphs: built for the members' buffer parities `key_cur` (and their
+  // complement, which the next step has) and active counts `key_active`
+  cudaGraphExec_t graph[2]{};
+  std::vector<mcv_handle *> key_hs;  // the handles with active members the graphs advance
+  std::vector<int> key_cur, key_active;
+};
+
+namespace {
+
+void drop_group_graphs(mcv_group *g) {
+  for (int c = 0; c < 2; ++c)
+    if (g->graph[c]) {
+      cudaGraphExecDestroy(g->graph[c]);
+      g->graph[c] = nullptr;
+    }
+}
+
+// One stage of the group's step (handles with active members only), with each
+// handle's buffer parity taken from curs.
+int enqueue_group_stage(mcv_group *g, const std::vector<mcv_handle *> &act, const std::vector<int> &curs, int s) {
+  const StageLauncher &L = act[0]->cands[g->cand];
+  StageBatch<kMaxGrids> b;
+  std::memset(&b, 0, sizeof(b));
+  for (size_t k = 0; k < act.size(); ++k)
+    if (int rc = add_grid(b, (int)k, act[k], L, s, curs[k])) return rc;
+  number_items(b, (int)act.size());
+  const int ctas = std::max(1, std::min(b.total, g->bps * act[0]->nsm));
+  L.launch_batch[stage_kind(act[0], s)](dim3(ctas), g->stream, b);
+  launch_halo_batch<kMaxGrids>(act.data(), curs.data(), (int)act.size(), s, g->stream);
+  return MCV_OK;
+}
+
+int build_group_graphs(mcv_group *g, const std::vector<mcv_handle *> &act) {
+  drop_group_graphs(g);
+  std::vector<int> curs(act.size());
+  for (size_t k = 0; k < act.size(); ++k) curs[k] = act[k]->mixed ? act[k]->cur : 0;
+  const bool mixed = act[0]->mixed;
+  for (int c = 0; c < (mixed ? 2 : 1); ++c) {
+    MCV_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal), "begin group capture");
+    int rc = MCV_OK;
+    for (int s = 0; s < num_stages(act[0]) && !rc; ++s) rc = enqueue_group_stage(g, act, curs, s);
+    cudaError_t le = cudaGetLastError();
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(g->stream, &graph);
+    if (rc || le != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc ? rc : cuda_fail(le, "launch during group capture");
+    }
+    MCV_CUDA(ce, "end group capture");
+    cudaError_t ie = cudaGraphInstantiate(&g->graph[c], graph, 0);
+    cudaGraphDestroy(graph);
+    MCV_CUDA(ie, "instantiate group graph");
+    for (int &x : curs) x = 1 - x;  // the next step reads the other buffers
+  }
+  g->key_hs = act;
+  g->key_cur.resize(act.size());
+  g->key_active.resize(act.size());
+  for (size_t k = 0; k < act.size(); ++k) {
+    g->key_cur[k] = act[k]->mixed ? act[k]->cur : 0;
+    g->key_active[k] = act[k]->n_active;
+  }
+  return MCV_OK;
+}
+
+// The handles a group step advances (those with active members) and the step
+// graph to replay first (0, or 1 when the parities are one step on), rebuilt
+// unless the handles, active counts and buffer parities are the ones the
+// graphs were built for.
+int prepare_group(mcv_group *g, std::vector<mcv_handle *> &act, int &flip) {
+  act.clear();
+  for (mcv_handle *h : g->hs) {
+    bool idle = false;
+    if (int rc = ready_to_step(h, &idle)) return rc;
+    if (!idle) act.push_back(h);
+  }
+  flip = 0;
+  if (act.empty()) return MCV_OK;
+  bool same = g->graph[0] && g->key_hs == act;
+  if (same) {
+    int eq = 1, cp = 1;
+    for (size_t k = 0; k < act.size(); ++k) {
+      const int c = act[k]->mixed ? act[k]->cur : 0;
+      same = same && g->key_active[k] == act[k]->n_active;
+      eq = eq && c == g->key_cur[k];
+      cp = cp && c == 1 - g->key_cur[k];
+    }
+    same = same && (eq || (cp && act[0]->mixed));
+    flip = eq ? 0 : 1;
+  }
+  if (!same) {
+    flip = 0;
+    return build_group_graphs(g, act);
+  }
+  return MCV_OK;
+}
+
+}  // namespace
+
+extern "C" int mcv_group_create(mcv_handle *const *handles, int count, int tile, mcv_group **out) {
+  if (!out) return fail(MCV_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!handles || count < 1 || count > kMaxGrids) return fail(MCV_ERR_ARG, "a group holds 1..4 handles");
+  for (int k = 0; k < count; ++k) {
+    const mcv_handle *h = handles[k];
+    if (!h) return fail(MCV_ERR_ARG, "handle is NULL");
+    for (int j = 0; j < k; ++j)
+      if (handles[j] == h) return fail(MCV_ERR_ARG, "a handle is listed twice");
+    if (h->order != handles[0]->order || h->precision != handles[0]->precision ||
+        h->scheme != handles[0]->scheme || h->device != handles[0]->device)
+      return fail(MCV_ERR_ARG, "the handles of a group share order, precision, scheme and device");
+  }
+  const int cand = tile >= 0 ? tile : handles[0]->choice;
+  if (cand < 0 || cand >= handles[0]->ncands || !handles[0]->cands[cand].tma)
+    return fail(MCV_ERR_ARG, "the group's stage-kernel candidate must be a persistent TMA form (mcv_tuning)");
+  mcv_group *g = new mcv_group();
+  g->hs.assign(handles, handles + count);
+  g->cand = cand;
+  g->bps = handles[0]->bps[cand];
+  cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming);
+  g->ready.assign(count, nullptr);
+  for (int k = 0; k < count && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&g->ready[k], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    mcv_group_destroy(g);
+    return cuda_fail(e, "group stream and events");
+  }
+  *out = g;
+  return MCV_OK;
+}
+
+extern "C" int mcv_group_step_async(mcv_group *g, int nsteps) {
+  if (!g) return fail(MCV_ERR_ARG, "group is NULL");
+  if (nsteps < 0) return fail(MCV_ERR_ARG, "nsteps must be >= 0");
+  std::vector<mcv_handle *> act;
+  int flip = 0;
+  if (int rc = prepare_group(g, act, flip)) return rc;
+  if (act.empty() || nsteps == 0) return MCV_OK;
+  // the group's stream runs after the work already queued on every handle's stream
+  for (size_t k = 0; k < g->hs.size(); ++k) {
+    MCV_CUDA(cudaEventRecord(g->ready[k], g->hs[k]->stream), "record handle event");
+    MCV_CUDA(cudaStreamWaitEvent(g->stream, g->ready[k], 0), "order group after handle");
+  }
+  int c = flip;
+  for (int it = 0; it < nsteps; ++it) {
+    MCV_CUDA(cudaGraphLaunch(g->graph[c], g->stream), "launch group graph");
+    if (act[0]->mixed) c = 1 - c;
+  }
+  // and every handle's later work runs after the group's
+  MCV_CUDA(cudaEventRecord(g->done, g->stream), "record group event");
+  for (mcv_handle *h : g->hs) MCV_CUDA(cudaStreamWaitEvent(h->stream, g->done, 0), "order handle after group");
+  for (mcv_handle *h : act) {
+    if (h->mixed && (nsteps % 2)) h->cur = 1 - h->cur;
+    for (int k = 0; k < h->n_active; ++k) {
+      const int m = h->active_host[k];
+      h->steps_done[m] += nsteps;
+      if (h->mixed) h->mcur[m] = h->cur;
+    }
+  }
+  return MCV_OK;
+}
+
+extern "C" int mcv_group_sync(mcv_group *g) {
+  if (!g) return fail(MCV_ERR_ARG, "group is NULL");
+  MCV_CUDA(cudaStreamSynchronize(g->stream), "group step");
+  for (mcv_handle *h : g->hs)
+    if (int rc = mcv_sync(h)) return rc;
+  return MCV_OK;
+}
+
+extern "C" int mcv_group_step(mcv_group *g, int nsteps) {
+  if (int rc = mcv_group_step_async(g, nsteps)) return rc;
+  return mcv_group_sync(g);
+}
+
+extern "C" int mcv_group_query(mcv_group *g) {
+  if (!g) return fail(MCV_ERR_ARG, "group is NULL");
+  const cudaError_t e = cudaStreamQuery(g->stream);
+  if (e == cudaSuccess) return MCV_OK;
+  if (e == cudaErrorNotReady) {
+    cudaGetLastError();
+    return MCV_BUSY;
+  }
+  return cuda_fail(e, "group query");
+}
+
+extern "C" int mcv_group_time_steps(mcv_group *g, int nsteps, double *ms) {
+  if (!g || nsteps < 1 || !ms) return fail(MCV_ERR_ARG, "group, nsteps >= 1 and ms required");
+  // graphs built and earlier work on the handles' streams done before timing
+  std::vector<mcv_handle *> act;
+  int flip = 0;
+  if (int rc = prepare_group(g, act, flip)) return rc;
+  for (mcv_handle *h : g->hs) MCV_CUDA(cudaStreamSynchronize(h->stream), "drain handle before timing");
+  cudaEvent_t e0, e1;
+  MCV_CUDA(cudaEventCreate(&e0), "event");
+  MCV_CUDA(cudaEventCreate(&e1), "event");
+  cudaEventRecord(e0, g->stream);
+  int rc = mcv_group_step_async(g, nsteps);
+  cudaEventRecord(e1, g->stream);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "timed group steps");
+  *ms = t;
+  return mcv_group_sync(g);
+}
+
+extern "C" int mcv_group_destroy(mcv_group *g) {
+  if (!g) return MCV_OK;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  drop_group_graphs(g);
+  for (cudaEvent_t e : g->ready)
+    if (e) cudaEventDestroy(e);
+  if (g->done) cudaEventDestroy(g->done);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
   return MCV_OK;
 }

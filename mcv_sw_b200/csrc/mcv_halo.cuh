@@ -75,19 +75,37 @@ __device__ __forceinline__ double ghost_interp(const double *q, double coef, dou
   }
 }
 
+// The grids one halo launch completes: one, or the grids of a batched stage
+// launch (each with its own threads, numbered from first[k]).
+template <int NB>
+struct HaloBatch {
+  GridDesc g[NB];
+  HaloArgs a[NB];
+  long long first[NB + 1];  // first thread of each grid
+  int ngrids;
+};
+
 // MIXED: the field completed is Y + increment.  Raw values combine Y with the
 // increment in FP64; the result minus Y at the destination is stored as the
 // new FP32 increment, so the next stage's input halo is the FP64 correction
 // of its own interior.
-template <int D, bool MIXED>
-__global__ void __launch_bounds__(128) halo_kernel(const GridDesc g, const HaloArgs a) {
+template <int D, bool MIXED, int NB>
+__global__ void __launch_bounds__(128) halo_kernel(const __grid_constant__ HaloBatch<NB> hb) {
   constexpr int H = D - 1;
-  const int n = g.n;
   // the next stage kernel may launch now: its items clear of the panel edges
   // read nothing this kernel writes, the others wait for its completion
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  // one thread per (member, panel, edge, halo line h = 0..H, position k)
-  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // one thread per (grid, member, panel, edge, halo line h = 0..H, position k)
+  long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= hb.first[hb.ngrids]) return;
+  int kg = 0;
+#pragma unroll
+  for (int j = 1; j < NB; ++j)
+    if (j < hb.ngrids && gid >= hb.first[j]) kg = j;
+  gid -= hb.first[kg];
+  const GridDesc &g = hb.g[kg];
+  const HaloArgs &a = hb.a[kg];
+  const int n = g.n;
   const long long per_member = 24LL * (H + 1) * n;
   if (gid >= per_member * a.members) return;
   const int slot = (int)(gid / per_member);

@@ -81,6 +81,27 @@ struct StageArgs {
   float wd, wt;  // increment = wd * (input increment) + wt * tendency (RK3/RK4 weights)
 };
 
+// The grids one stage launch advances: one (a handle's own step) or, in a
+// batched launch, up to kMaxGrids handles of the same order, arithmetic, tile
+// shape and stage kind, each with its own Nc, dt and members.  Work items of
+// the TMA form are numbered over all grids: first the items clear of the panel
+// edges of every grid (in grid order), then the edge items of every grid, so
+// that with programmatic dependent launch the edge-free items of every grid
+// start while the previous halo kernels still run.
+constexpr int kMaxGrids = 4;
+template <int NB>
+struct StageBatch {
+  TileMaps tm[NB];  // tensor maps of each grid's staged fields (TMA form)
+  GridDesc g[NB];
+  StageArgs a[NB];
+  int ngrids;
+  int total;        // work items of all grids
+  int nin;          // items clear of the panel edges, all grids
+  int in0[NB + 1];  // first edge-free item of each grid
+  int ed0[NB + 1];  // first edge item of each grid, counted from nin
+  int slots[NB];    // active members of each grid
+};
+
 // ---------------------------------------------------------------------------
 // One-dimensional MCV building blocks (src/spatial_operators_mod.F90:136-246).
 // Divisions by the cell width are multiplications by precomputed reciprocals,
@@ -478,6 +499,11 @@ __device__ __forceinline__ void mix_point(MixPoint &o, const double4 mx, const d
 struct WorkItem {
   int tx, ty, panel, slot;
 };
+// Edge-free items of one grid (tiles_x - 2)(tiles_y - 2) x 6 x nslots and its
+// edge items, each numbered from 0 (interior: j < nin x 6 x nslots).
+__host__ __device__ inline int edge_free_tiles(int tiles_x, int tiles_y) {
+  return (tiles_x > 2 ? tiles_x - 2 : 0) * (tiles_y > 2 ? tiles_y - 2 : 0);
+}
 __device__ __forceinline__ WorkItem decode_item(int wi, int tiles_x, int tiles_y, int nslots) {
   const int ix = max(tiles_x - 2, 0), iy = max(tiles_y - 2, 0);
   const int nin = ix * iy, nedge = tiles_x * tiles_y - nin;
@@ -509,6 +535,27 @@ __device__ __forceinline__ WorkItem decode_item(int wi, int tiles_x, int tiles_y
   return w;
 }
 
+// Work item wi of a (batched) TMA-form launch: its grid k and the item within
+// that grid (decode_item's numbering: edge-free items first).
+template <int NB>
+__device__ __forceinline__ WorkItem decode_batch(const StageBatch<NB> &b, int wi, int &k) {
+  k = 0;
+  int local;
+  if (wi < b.nin) {
+#pragma unroll
+    for (int j = 1; j < NB; ++j)
+      if (j < b.ngrids && wi >= b.in0[j]) k = j;
+    local = wi - b.in0[k];
+  } else {
+    const int e = wi - b.nin;
+#pragma unroll
+    for (int j = 1; j < NB; ++j)
+      if (j < b.ngrids && e >= b.ed0[j]) k = j;
+    local = (b.in0[k + 1] - b.in0[k]) + (e - b.ed0[k]);
+  }
+  return decode_item(local, b.g[k].tiles_x, b.g[k].tiles_y, b.slots[k]);
+}
+
 // PTX programmatic dependent launch: wait until the preceding kernel (the halo
 // kernel) has completed and its writes are visible; let the next kernel launch.
 __device__ __forceinline__ void wait_prerequisite_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
@@ -529,9 +576,8 @@ __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddep
 // linear references in the step's first stage and stores them, and the later
 // stages' copies bring them in with the tile.  Otherwise one CTA per (tile,
 // panel, member) loads its fields with ordinary loads.
-template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA, int OPT>
-__global__ void __launch_bounds__(NT, MINB)
-    stage_kernel(const GridDesc g, const StageArgs a, const __grid_constant__ TileMaps tm) {
+template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA, int OPT, int NB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__ StageBatch<NB> b) {
   using R = std::conditional_t<MIXED, float, double>;
   using T = Tile<D, CX, CY, R>;
   constexpr int H = T::H, LX = T::LX;
@@ -544,26 +590,29 @@ __global__ void __launch_bounds__(NT, MINB)
   double *qref = plane + 12;                                           // [3 points][3]
   int pb = 0;  // TMA form: plane buffer of the current work item
   uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + T::bar_off(MIXED));
-  const int ntile = g.tiles_x * g.tiles_y;
   // TMA form, loaded rows of 28..32 points: phase 0 maps lanes to columns
   constexpr bool ROWMAP = TMA && LX >= 28 && LX <= 32 && NT % 32 == 0;
   // number of staged fields (split precision: the first stage has no input increment)
   constexpr int NF = MIXED ? (first_stage(KIND) ? 4 : 7) : 8;
 
-  // TMA: issue the copies of work item wi's input fields (one thread)
-  const int nslots = tm.total / (ntile * 6);
-  // the loaded rectangle of tile (tx, ty) reaches a panel boundary line or the
-  // halo, which the previous halo kernel writes
-  auto touches_edge = [&](int tx, int ty) {
+  // the loaded rectangle of tile (tx, ty) of grid g reaches a panel boundary
+  // line or the halo, which the previous halo kernel writes
+  auto touches_edge = [&](const GridDesc &g, int tx, int ty) {
     const int cx = min(CX, g.Nc - tx * CX), cy = min(CY, g.Nc - ty * CY);
     const int x0 = tx * CX * (D - 1) - H, x1 = tx * CX * (D - 1) + cx * (D - 1) + H;  // interior indices
     const int y0 = ty * CY * (D - 1) - H, y1 = ty * CY * (D - 1) + cy * (D - 1) + H;
     return x0 < 1 || y0 < 1 || x1 > g.n - 2 || y1 > g.n - 2;
   };
   bool waited = false;  // TMA form, thread 0: the prerequisite grid has completed
+  // TMA: issue the copies of work item wi's input fields (one thread)
   auto issue = [&](int wi) {
-    const WorkItem it = decode_item(wi, g.tiles_x, g.tiles_y, nslots);
-    if (!waited && touches_edge(it.tx, it.ty)) {
+    int k;
+    const WorkItem it = decode_batch(b, wi, k);
+    const GridDesc &g = b.g[k];
+    const StageArgs &a = b.a[k];
+    const TileMaps &tm = b.tm[k];
+    const int ntile = g.tiles_x * g.tiles_y;
+    if (!waited && touches_edge(g, it.tx, it.ty)) {
       wait_prerequisite_grid();
       waited = true;
     }
@@ -595,9 +644,6 @@ __global__ void __launch_bounds__(NT, MINB)
                   a.prec + ((long long)(mem * 6 + panel) * ntile + it.ty * g.tiles_x + it.tx) * 12, 96u, bar);
     }
   };
-  // 1 / (full tile width in radians), x and y (split precision's linear references)
-  const double2 inv_full_w = MIXED ? make_double2(1. / ((double)CX * g.dx), 1. / ((double)CY * g.dx))
-                                   : make_double2(0., 0.);
   uint32_t parity = 0;
   if constexpr (TMA) {
     if (threadIdx.x == 0) {
@@ -605,10 +651,19 @@ __global__ void __launch_bounds__(NT, MINB)
       fence_mbar_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0 && (int)blockIdx.x < tm.total) issue(blockIdx.x);
+    if (threadIdx.x == 0 && (int)blockIdx.x < b.total) issue(blockIdx.x);
   }
-  const int wfirst = TMA ? (int)blockIdx.x : 0, wstep = TMA ? (int)gridDim.x : 1, wend = TMA ? tm.total : 1;
+  const int wfirst = TMA ? (int)blockIdx.x : 0, wstep = TMA ? (int)gridDim.x : 1, wend = TMA ? b.total : 1;
   for (int wi = wfirst; wi < wend; wi += wstep) {
+  int kgrid = 0;  // the item's grid
+  WorkItem item{};
+  if constexpr (TMA) item = decode_batch(b, wi, kgrid);
+  const GridDesc &g = b.g[kgrid];
+  const StageArgs &a = b.a[kgrid];
+  const int ntile = g.tiles_x * g.tiles_y;
+  // 1 / (full tile width in radians), x and y (split precision's linear references)
+  const double2 inv_full_w = MIXED ? make_double2(1. / ((double)CX * g.dx), 1. / ((double)CY * g.dx))
+                                   : make_double2(0., 0.);
   if constexpr (TMA && MIXED) {
     // alternate buffers: the next item's references (fitted by warp 0, or
     // copied in with the tile) land while other warps may still read this
@@ -620,7 +675,6 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   int tx, ty, panel, mem;
   if constexpr (TMA) {
-    const WorkItem item = decode_item(wi, g.tiles_x, g.tiles_y, nslots);
     tx = item.tx;
     ty = item.ty;
     panel = item.panel;
@@ -1421,18 +1475,19 @@ __global__ void __launch_bounds__(NT, MINB)
 // ---------------------------------------------------------------------------
 // Launch table of one tile shape (used by the tile-shape autotuner).
 // ---------------------------------------------------------------------------
-using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a,
-                               const TileMaps &tm);
+using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const StageBatch<1> &b);
+using StageBatchFn = void (*)(dim3 grid, cudaStream_t s, const StageBatch<kMaxGrids> &b);
 
 struct StageLauncher {
   int CX, CY, NT, minb;
   int walk;   // 0: sweeps as per-cell items; n: walks of n cells
   bool tma;   // persistent CTAs with TMA-staged tiles
   size_t smem;
-  int box_x, box_y;         // staged box of one field (TMA form)
-  StageLaunchFn launch[7];  // indexed by StageKind
-  cudaError_t (*prepare)(); // raises the dynamic shared-memory limit of every kind
-  int (*blocks_per_sm)();   // resident CTAs per SM (sizes the persistent grid)
+  int box_x, box_y;              // staged box of one field (TMA form)
+  StageLaunchFn launch[7];       // one grid, indexed by StageKind
+  StageBatchFn launch_batch[7];  // up to kMaxGrids grids in one launch (TMA form; else null)
+  cudaError_t (*prepare)();      // raises the dynamic shared-memory limit of every kind
+  int (*blocks_per_sm)();        // resident CTAs per SM (sizes the persistent grid)
 };
 
 template <int D, int CX, int CY, int NT, int MINB, bool MIXED, int WALK, bool TMA = false, int OPT = 0>
@@ -1445,8 +1500,8 @@ struct StageConfig {
   // launched with programmatic stream serialization: the kernel's CTAs may
   // become resident while the preceding halo kernel finishes (TMA form: items
   // clear of the panel edges also run then; the rest wait for it)
-  template <int KIND>
-  static void launch(dim3 grid, cudaStream_t s, const GridDesc &g, const StageArgs &a, const TileMaps &tm) {
+  template <int KIND, int NB>
+  static void launch_nb(dim3 grid, cudaStream_t s, const StageBatch<NB> &b) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(NT);
@@ -1457,14 +1512,26 @@ struct StageConfig {
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT>, g, a, tm);
+    cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, NB>, b);
+  }
+  template <int KIND>
+  static void launch(dim3 grid, cudaStream_t s, const StageBatch<1> &b) {
+    launch_nb<KIND, 1>(grid, s, b);
+  }
+  template <int KIND>
+  static void launch_batch(dim3 grid, cudaStream_t s, const StageBatch<kMaxGrids> &b) {
+    if constexpr (TMA) launch_nb<KIND, kMaxGrids>(grid, s, b);
   }
   template <int KIND>
   static cudaError_t attr() {
     // (the driver's own carveout choice: forcing the largest shared-memory
     // carveout shrank L1 and slowed the FP64 kernels by up to 20%)
-    return cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, 1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    if (e == cudaSuccess && TMA)
+      e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, kMaxGrids>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    return e;
   }
   static cudaError_t prepare() {
     cudaError_t e;
@@ -1473,19 +1540,30 @@ struct StageConfig {
       return e;
     return cudaSuccess;
   }
+  // resident CTAs per SM (the smaller of the one-grid and the batched forms)
   static int blocks_per_sm() {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT>, NT,
-                                                      SMEM) != cudaSuccess)
+    int n = 0, nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, 1>, NT, SMEM) != cudaSuccess)
       return 0;
-    return n;
+    if (TMA && cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                   &nb, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, kMaxGrids>, NT, SMEM) !=
+                   cudaSuccess)
+      return 0;
+    return TMA ? (nb < n ? nb : n) : n;
   }
   static StageLauncher make() {
     static_assert(SMEM <= 227 * 1024, "tile does not fit in shared memory");
     static_assert(MINB * (SMEM + 1024) <= 228 * 1024, "MINB tiles do not fit in one SM's shared memory");
-    return StageLauncher{CX,     CY,    NT,    MINB,  WALK, TMA, SMEM, T::BX, T::LY,
-                         {&launch<0>, &launch<1>, &launch<2>, &launch<3>, &launch<4>, &launch<5>, &launch<6>},
-                         &prepare, &blocks_per_sm};
+    StageLauncher L{CX, CY, NT, MINB, WALK, TMA, SMEM, T::BX, T::LY,
+                    {&launch<0>, &launch<1>, &launch<2>, &launch<3>, &launch<4>, &launch<5>, &launch<6>},
+                    {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr}, &prepare, &blocks_per_sm};
+    if constexpr (TMA) {
+      StageBatchFn fb[7] = {&launch_batch<0>, &launch_batch<1>, &launch_batch<2>, &launch_batch<3>,
+                            &launch_batch<4>, &launch_batch<5>, &launch_batch<6>};
+      for (int k = 0; k < 7; ++k) L.launch_batch[k] = fb[k];
+    }
+    return L;
   }
 };
 
