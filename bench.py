@@ -335,10 +335,16 @@ def serving_block(count, python_count, baseline_count):
                      "with mountains; RK3_TVD, CFL 0.45; geometry and initial states generated on the device at "
                      "admission"}
     if count > 0:
-        res, busy = serving.run_native(reqs[:count], precision="mixed", geoms=geoms)
+        # grouping: idle pools of one order whose grids lie in one factor-8
+        # size class advance together in one batched launch per stage
+        stats = {}
+        res, busy = serving.run_native(reqs[:count], precision="mixed", geoms=geoms, grouping=(4, 8.0),
+                                       stats_out=stats)
         out["native_server_mixed"] = dict(serving.summarize(res), max_concurrent_pools=busy,
+                                          chunks=stats.get("chunks"), grouped_chunks=stats.get("grouped_chunks"),
+                                          pools_created=stats.get("pools_created"),
                                           loop="mcv_server_submit_balanced_flow / mcv_server_poll / "
-                                               "mcv_server_result")
+                                               "mcv_server_result, grouping (4 grids, size class x8)")
     if python_count > 0:
         sub = reqs[:python_count]
         srv = serving.ForecastServer(precision="mixed", geoms=geoms, device_setup=True)

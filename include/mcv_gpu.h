@@ -345,6 +345,17 @@ int mcv_server_result(mcv_server *s, long long id, double *u, double *v, double 
  * created, pools evicted, chunks retired. */
 int mcv_server_stats(mcv_server *s, long long *stats);
 
+/* Grouping: pools of one order whose grids' step costs (points per member)
+ * fall in one bucket of a log scale of base max_cost_ratio form a class; a
+ * class's idle pools advance together, up to max_grids (1..4) pools per
+ * batched launch (mcv_group_*), and a pool whose class has a chunk on the GPU
+ * waits for it (at most one chunk) so that the class starts together.
+ * max_grids = 1 (the default): every pool on its own stream.  A grouped chunk
+ * takes the fewest steps any of its forecasts has left.  Pools whose
+ * stage-kernel candidate is not a persistent TMA form step alone.
+ * *grouped_chunks (may be NULL): grouped chunks launched so far. */
+int mcv_server_set_grouping(mcv_server *s, int max_grids, double max_cost_ratio, long long *grouped_chunks);
+
 /* Release every pool and the server (waits for queued work). */
 int mcv_server_destroy(mcv_server *s);
 

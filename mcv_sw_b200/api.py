@@ -120,6 +120,8 @@ def lib():
                                              ctypes.POINTER(ctypes.c_longlong), _I]),
         "mcv_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
         "mcv_server_destroy": (ctypes.c_int, [vp]),
+        "mcv_server_set_grouping": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double,
+                                                   ctypes.POINTER(ctypes.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -504,6 +506,14 @@ class Server:
                                        int(slot_bytes), int(max_slots), float(chunk_ms), int(tile), ctypes.byref(s)))
         self.s = s
         self.grids = {}  # request id -> (order, nc)
+
+    def set_grouping(self, max_grids=4, max_cost_ratio=4.0):
+        """Idle pools of one order whose step costs are within max_cost_ratio
+        advance together in one batched launch (max_grids pools; 1: off).
+        Returns the grouped chunks launched so far."""
+        n = ctypes.c_longlong()
+        _check(lib().mcv_server_set_grouping(self.s, int(max_grids), float(max_cost_ratio), ctypes.byref(n)))
+        return n.value
 
     def close(self):
         if getattr(self, "s", None):

@@ -64,6 +64,7 @@ struct Pool {
   long long in_flight = 0;  // steps of the chunk on the GPU (0: idle)
   double launched = 0.;
   double ms_per_step = -1.;  // measured, or < 0 before the first chunk
+  mcv_group *group = nullptr;  // the group whose launch holds the pool's chunk (null: its own stream)
 
   bool same_grid(int o, int n, double d) const { return order == o && nc == n && dt == d; }
   int free_slot() const {
@@ -90,6 +91,13 @@ struct mcv_server {
   std::map<long long, Finished> finished;
   std::deque<long long> unreported;  // finished ids not yet returned by mcv_server_poll
   long long pools_created = 0, pools_evicted = 0, chunks = 0;
+  // grouping: idle pools of one order whose per-member step costs fall in one
+  // bucket of a log scale of base group_ratio advance together, up to
+  // group_max per launch
+  int group_max = 1;
+  double group_ratio = 1.;
+  std::map<std::vector<mcv_handle *>, mcv_group *> groups;  // cached groups by pool handles
+  long long grouped_chunks = 0;
 };
 
 namespace {
@@ -108,6 +116,18 @@ int slots_for(const mcv_server *s, int order, int nc) {
   const long long per = footprint(s, order, nc, 2) - footprint(s, order, nc, 1);
   const long long n = s->slot_bytes / std::max(per, 1LL);
   return (int)std::max(1LL, std::min((long long)s->max_slots, n));
+}
+
+// Forget the cached groups that hold handle h (before its pool closes).
+void drop_groups_of(mcv_server *s, const mcv_handle *h) {
+  for (auto it = s->groups.begin(); it != s->groups.end();) {
+    if (std::find(it->first.begin(), it->first.end(), h) != it->first.end()) {
+      mcv_group_destroy(it->second);
+      it = s->groups.erase(it);
+    } else {
+      ++it;
+    }
+  }
 }
 
 void close_pool(Pool *p) {
@@ -140,6 +160,7 @@ Pool *new_pool(mcv_server *s, int order, int nc, double dt, int *rc) {
       if (!p->in_flight && p->empty() && (!victim || p->bytes > victim->bytes)) victim = p;
     if (!victim) return nullptr;
     s->pools.erase(std::find(s->pools.begin(), s->pools.end(), victim));
+    drop_groups_of(s, victim->h);
     close_pool(victim);
     ++s->pools_evicted;
   }
@@ -206,16 +227,31 @@ int admit(mcv_server *s, const Request &r, int *placed) {
   return MCV_OK;
 }
 
-long long chunk_steps(const mcv_server *s, const Pool *p) {
+// A pool's GPU time per step before its first chunk: ~1.3e-7 ms per point
+// and step for one member (B200); the grouping policy compares pools with it.
+double static_step_ms(const Pool *p) {
+  const double n = 6. * std::pow((double)p->nc * (p->order - 1) + 1., 2.);
+  return std::max(1.3e-7 * n * (double)p->active.size(), 0.02);
+}
+
+double step_ms(const Pool *p) { return p->ms_per_step > 0. ? p->ms_per_step : static_step_ms(p); }
+
+// Grouping class of a pool: its order and its step cost's bucket on a
+// log scale of base group_ratio (pools of one class step in lockstep).
+long long group_class(const mcv_server *s, const Pool *p) {
+  const double points = 6. * std::pow((double)p->nc * (p->order - 1) + 1., 2.);  // per member
+  const long long b = (long long)std::floor(std::log(points) / std::log(std::max(s->group_ratio, 1.0001)));
+  return (long long)p->order * 1000000 + b;
+}
+
+long long steps_left(const Pool *p) {
   long long left = p->left[p->active[0]];
   for (int slot : p->active) left = std::min(left, p->left[slot]);
-  double est = p->ms_per_step;
-  if (est <= 0.) {
-    // before the first chunk: ~1.3e-7 ms per point and step for one member (B200)
-    const double n = 6. * std::pow((double)p->nc * (p->order - 1) + 1., 2.);
-    est = std::max(1.3e-7 * n * (double)p->active.size(), 0.02);
-  }
-  return std::max(1LL, std::min(left, (long long)(s->chunk_ms / est)));
+  return left;
+}
+
+long long chunk_steps(const mcv_server *s, const Pool *p) {
+  return std::max(1LL, std::min(steps_left(p), (long long)(s->chunk_ms / step_ms(p))));
 }
 
 // Record request `id` as failed with status rc (its result call reports rc).
@@ -236,6 +272,7 @@ void fail_request(mcv_server *s, long long id, long long nsteps, int rc) {
 int finish_chunk(mcv_server *s, Pool *p) {
   const long long steps = p->in_flight;
   p->in_flight = 0;
+  p->group = nullptr;
   ++s->chunks;
   const double el = (now_ms() - p->launched) / (double)steps;
   p->ms_per_step = p->ms_per_step < 0. ? el : 0.5 * (p->ms_per_step + el);
@@ -399,12 +436,13 @@ extern "C" int mcv_server_poll(mcv_server *s, long long *ids, int max_ids, int *
   int chunk_err = MCV_OK;
   for (Pool *p : s->pools) {
     if (!p->in_flight) continue;
-    const int q = mcv_query(p->h);
+    const int q = p->group ? mcv_group_query(p->group) : mcv_query(p->h);
     if (q == MCV_BUSY) continue;
     const int rc = (q != MCV_OK) ? q : finish_chunk(s, p);
     if (q != MCV_OK) {
       // the chunk's work is lost: its forecasts fail and their slots free up
       p->in_flight = 0;
+      p->group = nullptr;
       for (int slot : p->active) {
         fail_request(s, p->req[slot], p->total[slot], q);
         p->req[slot] = -1;
@@ -427,31 +465,100 @@ extern "C" int mcv_server_poll(mcv_server *s, long long *ids, int max_ids, int *
     }
     it = placed ? s->waiting.erase(it) : std::next(it);
   }
-  // 3. the next chunk of every idle pool with active slots
+  // 3. the next chunk of every idle pool with active slots: alone on its
+  // own stream, or (grouping) together with the idle pools of its class
+  // (order and step-cost bucket), in one batched launch per stage
+  auto fail_pool = [&](Pool *p, int rc) {
+    // the pool cannot step: its forecasts fail and their slots free up
+    for (int slot : p->active) {
+      fail_request(s, p->req[slot], p->total[slot], rc);
+      p->req[slot] = -1;
+    }
+    p->active.clear();
+    if (!first) first = rc;
+  };
+  std::vector<Pool *> ready;
   for (Pool *p : s->pools) {
     if (p->in_flight || p->active.empty()) continue;
-    int rc = MCV_OK;
     if (!p->dev_active_set || p->dev_active != p->active) {
-      rc = mcv_set_active(p->h, (int)p->active.size(), p->active.data());
-      if (!rc) {
-        p->dev_active = p->active;
-        p->dev_active_set = true;
+      if (int rc = mcv_set_active(p->h, (int)p->active.size(), p->active.data())) {
+        fail_pool(p, rc);
+        continue;
+      }
+      p->dev_active = p->active;
+      p->dev_active_set = true;
+    }
+    ready.push_back(p);
+  }
+  if (s->group_max > 1) {
+    // a pool whose class has a chunk on the GPU waits for it (at most one
+    // chunk), so that the class's pools start their chunks together
+    std::vector<long long> busy;
+    for (const Pool *q : s->pools)
+      if (q->in_flight) busy.push_back(group_class(s, q));
+    ready.erase(std::remove_if(ready.begin(), ready.end(),
+                               [&](const Pool *p) {
+                                 return std::find(busy.begin(), busy.end(), group_class(s, p)) != busy.end();
+                               }),
+                ready.end());
+  }
+  std::stable_sort(ready.begin(), ready.end(), [&](const Pool *a, const Pool *b) {
+    return group_class(s, a) < group_class(s, b);
+  });
+  for (size_t i = 0; i < ready.size();) {
+    size_t j = i + 1;
+    if (s->group_max > 1)
+      while (j < ready.size() && (int)(j - i) < s->group_max && group_class(s, ready[j]) == group_class(s, ready[i]))
+        ++j;
+    mcv_group *grp = nullptr;
+    if (j - i > 1) {
+      std::vector<mcv_handle *> hs;
+      for (size_t k = i; k < j; ++k) hs.push_back(ready[k]->h);
+      auto it = s->groups.find(hs);
+      if (it != s->groups.end()) {
+        grp = it->second;
+      } else if (mcv_group_create(hs.data(), (int)hs.size(), s->tile, &grp) == MCV_OK) {
+        s->groups[hs] = grp;
+      } else {
+        grp = nullptr;  // (e.g. a pool's candidate is not a persistent TMA form): each pool alone
       }
     }
-    const long long k = chunk_steps(s, p);
-    p->launched = now_ms();
-    if (!rc) rc = mcv_step_async(p->h, (int)k);
-    if (rc) {
-      // the pool cannot step: its forecasts fail and their slots free up
-      for (int slot : p->active) {
-        fail_request(s, p->req[slot], p->total[slot], rc);
-        p->req[slot] = -1;
+    if (!grp) {
+      for (size_t k = i; k < j; ++k) {
+        Pool *p = ready[k];
+        const long long steps = chunk_steps(s, p);
+        p->launched = now_ms();
+        if (int rc = mcv_step_async(p->h, (int)steps)) {
+          fail_pool(p, rc);
+          continue;
+        }
+        p->in_flight = steps;
       }
-      p->active.clear();
-      if (!first) first = rc;
+      i = j;
       continue;
     }
-    p->in_flight = k;
+    // one chunk for the group: the fewest steps any of its forecasts has left,
+    // within chunk_ms of the pools' summed step times
+    long long steps = steps_left(ready[i]);
+    double ms = 0.;
+    for (size_t k = i; k < j; ++k) {
+      steps = std::min(steps, steps_left(ready[k]));
+      ms += step_ms(ready[k]);
+    }
+    steps = std::max(1LL, std::min(steps, (long long)(s->chunk_ms / ms)));
+    const double t = now_ms();
+    if (int rc = mcv_group_step_async(grp, (int)steps)) {
+      for (size_t k = i; k < j; ++k) fail_pool(ready[k], rc);
+      i = j;
+      continue;
+    }
+    ++s->grouped_chunks;
+    for (size_t k = i; k < j; ++k) {
+      ready[k]->launched = t;
+      ready[k]->in_flight = steps;
+      ready[k]->group = grp;
+    }
+    i = j;
   }
   // 4. the forecasts finished (or failed) since the last poll
   while (*n_ids < max_ids && !s->unreported.empty()) {
@@ -523,8 +630,23 @@ extern "C" int mcv_server_stats(mcv_server *s, long long *stats) {
   return MCV_OK;
 }
 
+extern "C" int mcv_server_set_grouping(mcv_server *s, int max_grids, double max_cost_ratio,
+                                       long long *grouped_chunks) {
+  if (!s) return fail(MCV_ERR_ARG, "server is NULL");
+  if (max_grids < 1 || max_grids > 4 || !(max_cost_ratio >= 1.))
+    return fail(MCV_ERR_ARG, "max_grids must be 1..4 and max_cost_ratio >= 1");
+  s->group_max = max_grids;
+  s->group_ratio = max_cost_ratio;
+  if (grouped_chunks) *grouped_chunks = s->grouped_chunks;
+  return MCV_OK;
+}
+
 extern "C" int mcv_server_destroy(mcv_server *s) {
   if (!s) return MCV_OK;
+  for (Pool *p : s->pools)
+    if (p->h) mcv_sync(p->h);
+  for (auto &kv : s->groups) mcv_group_destroy(kv.second);
+  s->groups.clear();
   for (Pool *p : s->pools) close_pool(p);
   delete s;
   return MCV_OK;

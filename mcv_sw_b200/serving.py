@@ -391,15 +391,18 @@ def run_one_at_a_time(requests, precision="fp64", scheme="RK3_TVD", radius=cases
 
 def run_native(requests, precision="mixed", scheme="RK3_TVD", radius=cases.EARTH_RADIUS, tile=-1, chunk_ms=25.0,
                hbm_budget=0, slot_bytes=8e9, max_slots=32, keep_states=False, geoms=None, prepare=True,
-               poll_s=2e-4, clock=time.perf_counter):
+               poll_s=2e-4, clock=time.perf_counter, grouping=None, stats_out=None):
     """Serve `requests` with the native server (mcv_server_*): each request is
     submitted at its arrival time, with the dt and step count ForecastServer
-    gives it, and the loop polls until every forecast is back.  Returns the
+    gives it, and the loop polls until every forecast is back.  grouping:
+    (max_grids, max_cost_ratio) of mcv_server_set_grouping, or None (off).  Returns the
     Results in input order (`admitted` is the submission time) and the
     largest number of pools seen with a chunk on the GPU at once."""
     policy = ForecastServer(precision=precision, scheme=scheme, hbm_budget=1 << 62, radius=radius, geoms=geoms)
     results, by_id, busy_max = {}, {}, 0
     with api.Server(precision, scheme, radius, int(hbm_budget), int(slot_bytes), max_slots, chunk_ms, tile) as srv:
+        if grouping:
+            srv.set_grouping(*grouping)
         if prepare:
             for key in sorted({r.key for r in requests}):
                 srv.prepare(key[0], key[1], policy.group_dt(key))
@@ -427,6 +430,10 @@ def run_native(requests, precision="mixed", scheme="RK3_TVD", radius=cases.EARTH
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - (clock() - t0))))
                 else:
                     time.sleep(poll_s)
+        if stats_out is not None:
+            stats_out.update(srv.stats())
+            if grouping:
+                stats_out["grouped_chunks"] = srv.set_grouping(*grouping)
     return [results[r.id] for r in requests], busy_max
 
 

@@ -148,4 +148,49 @@ int mcv_destroy(mcv_handle *h) {
   return MCV_OK;
 }
 
+// A fake group steps its handles' active members together; its chunk
+// completes after two mcv_group_query calls, during which its handles are busy.
+}  // extern "C"
+struct mcv_group {
+  std::vector<mcv_handle *> hs;
+  int pending = 0;
+};
+int g_live_groups = 0;
+long long g_group_steps = 0;
+extern "C" {
+
+int mcv_group_create(mcv_handle *const *handles, int count, int, mcv_group **out) {
+  if (count < 1 || count > 4) return mcv::fail(MCV_ERR_ARG, "bad group");
+  mcv_group *g = new mcv_group();
+  g->hs.assign(handles, handles + count);
+  *out = g;
+  ++g_live_groups;
+  return MCV_OK;
+}
+
+int mcv_group_step_async(mcv_group *g, int nsteps) {
+  for (mcv_handle *h : g->hs)
+    if (h->pending) return mcv::fail(MCV_ERR_ORDER, "group step on a busy handle");
+  for (mcv_handle *h : g->hs) {
+    for (int m : h->active) h->steps[m] += nsteps;
+    h->pending = 1000000;  // busy until the group completes
+  }
+  g->pending = 2;
+  ++g_group_steps;
+  return MCV_OK;
+}
+
+int mcv_group_query(mcv_group *g) {
+  if (g->pending > 0 && --g->pending > 0) return MCV_BUSY;
+  for (mcv_handle *h : g->hs) h->pending = 0;
+  return MCV_OK;
+}
+
+int mcv_group_destroy(mcv_group *g) {
+  for (mcv_handle *h : g->hs) h->pending = 0;
+  delete g;
+  --g_live_groups;
+  return MCV_OK;
+}
+
 }  // extern "C"

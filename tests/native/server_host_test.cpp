@@ -11,6 +11,8 @@
 
 extern int g_live_handles;
 extern long long g_created;
+extern int g_live_groups;
+extern long long g_group_steps;
 
 #define CHECK(c)                                              \
   do {                                                        \
@@ -199,6 +201,26 @@ int main() {
     CHECK(st[0] == 0 && st[1] == 0 && st[2] == 0);
     CHECK(mcv_server_destroy(s) == MCV_OK);
     CHECK(g_live_handles == 0);
+  }
+  {
+    // grouping: pools of one order with close step costs advance together in
+    // one group chunk; every forecast still gets exactly its steps
+    mcv_server *s = nullptr;
+    CHECK(mcv_server_create(MCV_MIXED, MCV_RK3_TVD, 6.371e6, 1LL << 40, 2400, 32, 0.1, 0, &s) == MCV_OK);
+    long long gc = -1;
+    CHECK(mcv_server_set_grouping(s, 0, 2., &gc) == MCV_ERR_ARG);
+    CHECK(mcv_server_set_grouping(s, 3, 4., &gc) == MCV_OK && gc == 0);
+    std::map<long long, Expect> want;
+    const int ncs[] = {4, 5, 6, 4, 5, 6, 5, 4};
+    const long long steps[] = {9, 4, 13, 2, 7, 5, 11, 3};
+    for (int i = 0; i < 8; ++i) CHECK(submit_host(s, 3, ncs[i], 100., steps[i], 50. + i, want) == 0);
+    CHECK(submit_host(s, 4, 4, 100., 6, 70., want) == 0);  // another order: never grouped with the others
+    const long long group_steps0 = g_group_steps;
+    CHECK(drain(s, want, st) == 0);
+    CHECK(g_group_steps > group_steps0);
+    CHECK(mcv_server_set_grouping(s, 3, 4., &gc) == MCV_OK && gc == g_group_steps - group_steps0);
+    CHECK(mcv_server_destroy(s) == MCV_OK);
+    CHECK(g_live_handles == 0 && g_live_groups == 0);
   }
   std::printf("ok\n");
   return 0;

@@ -159,3 +159,29 @@ def test_device_admission_stream():
     for k in ("u", "v", "phi"):
         a, b = dev.state[k][:, H:H + n, H:H + n], host.state[k][:, H:H + n, H:H + n]
         assert np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)) <= 1e-12, k
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_grouped_native_server_matches_the_request_loop(precision):
+    """With grouping, pools of different Nc advance in one batched launch per
+    stage (mcv_group_*); every forecast is still the one the request loop gives
+    it on the same tile shape and device-built geometry, bit for bit, and the
+    one the native loop gives it without grouping.  Candidate 6 is a persistent
+    TMA form for both orders; the requests all arrive at once, so the pools of
+    the MCV3 grids (Nc 8 and 12, one size class) start together."""
+    reqs, geoms = stream()
+    for r in reqs:
+        r.arrival = 0.0
+    kw = dict(precision=precision, tile=6, keep_states=True, geoms=geoms, hbm_budget=4 << 30,
+              slot_bytes=64 << 20, chunk_ms=0.5)
+    py = serving.ForecastServer(device_setup=True, **kw)
+    a = py.run(reqs)
+    py.close()
+    plain, _ = serving.run_native(reqs, **kw)
+    stats = {}
+    b, busy = serving.run_native(reqs, grouping=(4, 16.0), stats_out=stats, **kw)
+    assert stats["grouped_chunks"] > 0
+    for req, x, y, z in zip(reqs, a, b, plain):
+        assert y.finite and x.nsteps == y.nsteps
+        assert same(x, y), req.id
+        assert same(z, y), req.id
