@@ -342,6 +342,9 @@ HaloArgs halo_args(mcv_handle *h, int s, int c) {
   a.dx = h->g.dx;
   a.dx2 = h->dx2;
   a.dx3 = h->dx3;
+  a.rdx = 1. / h->g.dx;
+  a.rdx2 = 1. / h->dx2;
+  a.r2dx3 = 1. / (2. * h->dx3);
   a.members = h->n_active;
   a.active = h->active;
   const int kind = stage_kind(h, s);
@@ -369,19 +372,21 @@ template <int NB>
 void launch_halo_batch(mcv_handle *const *hs, const int *curs, int count, int s, cudaStream_t st) {
   HaloBatch<NB> b;
   std::memset(&b, 0, sizeof(b));
-  long long threads = 0;
+  int slots = 0, nmax = 0;
   for (int k = 0; k < count; ++k) {
     mcv_handle *h = hs[k];
     b.g[k] = h->g;
     b.a[k] = halo_args(h, s, curs[k]);
-    b.first[k] = threads;
-    threads += 24LL * (h->H + 1) * h->g.n * h->n_active;
+    b.first[k] = slots;
+    slots += h->n_active;
+    nmax = std::max(nmax, h->g.n);
   }
-  b.first[count] = threads;
+  b.first[count] = slots;
   b.ngrids = count;
   const bool mixed_inc = hs[0]->mixed && !last_stage(stage_kind(hs[0], s));
   const int block = 128;
-  const unsigned grid = (unsigned)((threads + block - 1) / block);
+  // x: positions along an edge; y: 4 edges x 6 panels x (H+1) lines; z: grids' active members
+  const dim3 grid((unsigned)((nmax + block - 1) / block), (unsigned)(24 * (hs[0]->H + 1)), (unsigned)slots);
   if (hs[0]->order == 3) {
     if (mixed_inc) halo_kernel<3, true, NB><<<grid, block, 0, st>>>(b);
     else halo_kernel<3, false, NB><<<grid, block, 0, st>>>(b);

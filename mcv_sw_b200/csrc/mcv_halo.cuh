@@ -13,6 +13,7 @@ struct HaloArgs {
   const int *giref;           // ghost%iref [H][n] (1-based cell)
   const double2 *gcoef;       // {ghost%coef, ghost%coef**3.} [H][n]
   double dx, dx2, dx3;        // dx, dx**2., dx**3.
+  double rdx, rdx2, r2dx3;    // 1/dx, 1/dx**2., 1/(2 dx**3.)
   int members;                // active members in this launch
   const int *active;          // member index of each active slot [members]
   // split precision: the field completed is Y + increment; u/v/phi above are
@@ -61,17 +62,19 @@ __device__ __forceinline__ int boundary_slot(int i, int j, int n) {
   return 1 * n + j;
 }
 
-// linear_interp, src/ghost_mod.f90:183-227
+// linear_interp, src/ghost_mod.f90:183-227.  The divisions by dx, dx**2 and
+// 2 dx**3 are multiplications by their reciprocals (one rounding away from
+// the reference's quotients, as the stage kernel's cell widths are).
 template <int D>
-__device__ __forceinline__ double ghost_interp(const double *q, double coef, double coef3, double dx, double dx2,
-                                               double dx3) {
+__device__ __forceinline__ double ghost_interp(const double *q, double coef, double coef3, const HaloArgs &a) {
   if constexpr (D == 3) {
-    return q[0] - (3. * q[0] - 4. * q[1] + q[2]) * coef / dx + 2. * (q[0] - 2. * q[1] + q[2]) * (coef * coef) / dx2;
+    return q[0] - (3. * q[0] - 4. * q[1] + q[2]) * coef * a.rdx +
+           2. * (q[0] - 2. * q[1] + q[2]) * (coef * coef) * a.rdx2;
   } else {
-    return (2. * dx3 * q[0] + dx2 * (-(11. * q[0]) + 18. * q[1] - 9. * q[2] + 2. * q[3]) * coef +
-            9. * dx * (2. * q[0] - 5. * q[1] + 4. * q[2] - q[3]) * (coef * coef) +
-            9. * (-q[0] + 3. * q[1] - 3. * q[2] + q[3]) * coef3) /
-           (2. * dx3);
+    return (2. * a.dx3 * q[0] + a.dx2 * (-(11. * q[0]) + 18. * q[1] - 9. * q[2] + 2. * q[3]) * coef +
+            9. * a.dx * (2. * q[0] - 5. * q[1] + 4. * q[2] - q[3]) * (coef * coef) +
+            9. * (-q[0] + 3. * q[1] - 3. * q[2] + q[3]) * coef3) *
+           a.r2dx3;
   }
 }
 
@@ -81,7 +84,7 @@ template <int NB>
 struct HaloBatch {
   GridDesc g[NB];
   HaloArgs a[NB];
-  long long first[NB + 1];  // first thread of each grid
+  int first[NB + 1];  // first member slot (blockIdx.z) of each grid
   int ngrids;
 };
 
@@ -95,27 +98,24 @@ __global__ void __launch_bounds__(128) halo_kernel(const __grid_constant__ HaloB
   // the next stage kernel may launch now: its items clear of the panel edges
   // read nothing this kernel writes, the others wait for its completion
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  // one thread per (grid, member, panel, edge, halo line h = 0..H, position k)
-  long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= hb.first[hb.ngrids]) return;
+  // one thread per (position k along the edge: x; panel, edge and halo line
+  // h = 0..H: y; grid and active member: z) -- no runtime divisions before
+  // the first loads
+  const int z = blockIdx.z;
   int kg = 0;
 #pragma unroll
   for (int j = 1; j < NB; ++j)
-    if (j < hb.ngrids && gid >= hb.first[j]) kg = j;
-  gid -= hb.first[kg];
+    if (j < hb.ngrids && z >= hb.first[j]) kg = j;
   const GridDesc &g = hb.g[kg];
   const HaloArgs &a = hb.a[kg];
   const int n = g.n;
-  const long long per_member = 24LL * (H + 1) * n;
-  if (gid >= per_member * a.members) return;
-  const int slot = (int)(gid / per_member);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int slot = z - hb.first[kg];
   const int mem = __ldg(a.active + slot);
-  int rem = (int)(gid - (long long)slot * per_member);
-  const int k = rem % n;
-  rem /= n;
-  const int h = rem % (H + 1);
-  const int pe = rem / (H + 1);
-  const int p = pe / 4, e = pe % 4;
+  const int h = blockIdx.y % (H + 1);
+  const int pe = blockIdx.y / (H + 1);
+  const int p = pe >> 2, e = pe & 3;
   const EdgeLink L = c_links[p][e];
   const int q = L.q, e2 = L.e2;
   const long long mb = (long long)mem * g.mstride;
@@ -202,9 +202,9 @@ __global__ void __launch_bounds__(128) halo_kernel(const __grid_constant__ HaloB
       qm[m] = M[m].y * su + M[m].w * sv;
       qp[m] = sp;
     }
-    zw = ghost_interp<D>(qz, cc.x, cc.y, a.dx, a.dx2, a.dx3);
-    mw = ghost_interp<D>(qm, cc.x, cc.y, a.dx, a.dx2, a.dx3);
-    ph = ghost_interp<D>(qp, cc.x, cc.y, a.dx, a.dx2, a.dx3);
+    zw = ghost_interp<D>(qz, cc.x, cc.y, a);
+    mw = ghost_interp<D>(qm, cc.x, cc.y, a);
+    ph = ghost_interp<D>(qp, cc.x, cc.y, a);
   } else if (k > 0 && k < n - 1) {
     // boundary line: edge average (spatial_operators_mod.F90:298-345)
     const int ks = L.rev ? n - 1 - k : k;
