@@ -162,6 +162,7 @@ int mcv_selftest_wait(int complete, double limit_ms, int *timed_out, double *ela
  * bit for bit that of the handle stepped alone on the same candidate.  The
  * handles keep working alone as well: the group orders its work after what
  * is queued on their streams, and their later work after the group's.
+ * Destroy a group before any of its handles.
  * ------------------------------------------------------------------- */
 typedef struct mcv_group mcv_group;
 int mcv_group_create(mcv_handle *const *handles, int count, int tile, mcv_group **out);

@@ -1586,6 +1586,7 @@ struct mcv_group {
 namespace {
 
 void drop_group_graphs(mcv_group *g) {
+  if (g->graph[0] || g->graph[1]) cudaStreamSynchronize(g->stream);  // launches still queued end first
   for (int c = 0; c < 2; ++c)
     if (g->graph[c]) {
       cudaGraphExecDestroy(g->graph[c]);
