@@ -239,6 +239,27 @@ __device__ __forceinline__ void cell_derivs2(float2 out[D], const float2 *f, con
   }
 }
 
+// Interface eigenvalues or upwind signs along a walk, interface i = 0..ncells:
+// read from an array (ArrLam), or formed at the interface point from the
+// stored contravariant wind c and G^ii phi (EigLam: max(|c - s|, |c + s|) =
+// |c| + s with s = sqrt(G^ii phi), spatial_operators_mod.F90:248-280; SgnLam:
+// the upwind sign of c, :83-85), st = the interface points' stride.
+template <typename R>
+struct ArrLam {
+  const R *p;
+  __device__ __forceinline__ R operator()(int i) const { return p[i]; }
+};
+struct EigLam {
+  const float *c, *gp;
+  int st;
+  __device__ __forceinline__ float operator()(int i) const { return fabsf(c[i * st]) + sqrtf(gp[i * st]); }
+};
+struct SgnLam {
+  const float *c;
+  int st;
+  __device__ __forceinline__ float operator()(int i) const { return (c[i * st] < 0.f) ? -1.f : 1.f; }
+};
+
 // calc_tendP (src/spatial_operators_mod.F90:136-202) applied to every cell of
 // one grid line of `ncells` cells, as the x-sweep (:63-93) and y-sweep (:95-125)
 // do for each row and column.  f and q point to the first point of the halo
@@ -250,8 +271,8 @@ __device__ __forceinline__ void cell_derivs2(float2 out[D], const float2 *f, con
 // The walk's last point is written only when the walk ends the line (`ends`):
 // otherwise it is the next walk's first point, which that walk writes (one
 // writer per point).
-template <int D, int NMAX, int S, int OS, bool SAME, typename R>
-__device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, int ncells, bool ends, R *out,
+template <int D, int NMAX, int S, int OS, bool SAME, typename R, class L>
+__device__ __forceinline__ void line_walk(const R *f, const R *q, const L &lam, int ncells, bool ends, R *out,
                                           const Widths<R> &w) {
   const R ip = (D == 3) ? w.inv_dx : w.inv_2dx;
   R cf[D], cq[D];
@@ -279,7 +300,7 @@ __device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, 
     }
   }
   R fL = polyfit_left<D>(cf, ip), qL = SAME ? fL : polyfit_left<D>(cq, ip);
-  R fluxL = riemann(fR, fL, qR, qL, lam[0]);
+  R fluxL = riemann(fR, fL, qR, qL, lam(0));
   fR = polyfit_right<D>(cf, ip);
   qR = SAME ? fR : polyfit_right<D>(cq, ip);
 #pragma unroll
@@ -294,7 +315,7 @@ __device__ __forceinline__ void line_walk(const R *f, const R *q, const R *lam, 
         nq[m] = SAME ? nf[m] : q[((c + 2) * (D - 1) + m) * S];
       }
       const R nfL = polyfit_left<D>(nf, ip), nqL = SAME ? nfL : polyfit_left<D>(nq, ip);
-      const R fluxR = riemann(fR, nfL, qR, nqL, lam[c + 1]);
+      const R fluxR = riemann(fR, nfL, qR, nqL, lam(c + 1));
       R o[D];
       o[0] = fluxL;
       o[D - 1] = fluxR;
@@ -342,8 +363,8 @@ __device__ __forceinline__ void cell_interior2(float2 o[D], const float2 *c, con
 // line_walk for two quantities at once (packed FP32 pairs, one eigenvalue per
 // interface): f and q point to the first point of the halo cell before the
 // walk, results go to outx (first of the pair) and outy (second).
-template <int D, int NMAX, int S, int OS>
-__device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, const float *lam, int ncells, bool ends,
+template <int D, int NMAX, int S, int OS, class L>
+__device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, const L &lam, int ncells, bool ends,
                                            float *outx, float *outy, const Widths<float> &w) {
   const float2 ip = bc2((D == 3) ? w.inv_dx : w.inv_2dx);
   float2 cf[D], cq[D];
@@ -360,7 +381,7 @@ __device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, con
     cf[m] = f[(D - 1 + m) * S];
     cq[m] = q[(D - 1 + m) * S];
   }
-  float2 fluxL = riemann2(fR, polyfit_left2<D>(cf, ip), qR, polyfit_left2<D>(cq, ip), lam[0]);
+  float2 fluxL = riemann2(fR, polyfit_left2<D>(cf, ip), qR, polyfit_left2<D>(cq, ip), lam(0));
   fR = polyfit_right2<D>(cf, ip);
   qR = polyfit_right2<D>(cq, ip);
 #pragma unroll
@@ -374,7 +395,7 @@ __device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, con
         nf[m] = f[((c + 2) * (D - 1) + m) * S];
         nq[m] = q[((c + 2) * (D - 1) + m) * S];
       }
-      const float2 fluxR = riemann2(fR, polyfit_left2<D>(nf, ip), qR, polyfit_left2<D>(nq, ip), lam[c + 1]);
+      const float2 fluxR = riemann2(fR, polyfit_left2<D>(nf, ip), qR, polyfit_left2<D>(nq, ip), lam(c + 1));
       float2 o[D];
       o[0] = fluxL;
       o[D - 1] = fluxR;
@@ -422,13 +443,16 @@ struct Tile {
   // ... interior-only arrays: sqrtG, cU, cV (split precision: 1/sqrtG, cU,
   // cV, sqrtG f) ...
   static constexpr int SG = (PAIRED ? 10 : 6) * A, CU = SG + I, CV = CU + I, FC = CV + I;
-  // ... interface eigenvalues and upwind signs ...
+  // ... interface eigenvalues and upwind signs (FP64 policy); split precision
+  // keeps G^11 phi and G^22 phi per interior point (GPX, GPY) instead and
+  // forms the eigenvalues and signs in the sweeps ...
   static constexpr int LAMX = CV + (PAIRED ? 2 : 1) * I;  // [TY][CX+1]
   static constexpr int SGNX = LAMX + TY * (CX + 1);
   static constexpr int LAMY = SGNX + TY * (CX + 1);  // [TX][CY+1]
   static constexpr int SGNY = LAMY + TX * (CY + 1);
+  static constexpr int GPX = LAMX, GPY = LAMX + I;  // split precision [TY][TX] each
   // ... sweep results [3][TY][TX] each ...
-  static constexpr int XR = SGNY + TX * (CY + 1);
+  static constexpr int XR = PAIRED ? GPY + I : SGNY + TX * (CY + 1);
   static constexpr int YR = XR + 3 * I;
   static constexpr int TOTAL = YR + 3 * I;
   // split precision, after the R arrays: 1-D metric tables [LX] and [LY] double4,
@@ -831,7 +855,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
       sm[T::SG + ii] = sg;
       sm[T::CU + ii] = cu;
       sm[T::CV + ii] = cv;
-      if constexpr (MIXED) sm[T::FC + ii] = fc;
+      if constexpr (MIXED) {
+        // the sweeps form the interface eigenvalues and signs from these
+        sm[T::FC + ii] = fc;
+        sm[T::GPX + ii] = g11 * phi;
+        sm[T::GPY + ii] = g22 * phi;
+        return;
+      }
       // max(|c - s|, |c + s|) with s = sqrt(G^ii phi) >= 0 is exactly |c| + s
       if (ix % (D - 1) == 0) {
         sm[T::LAMX + iy * (CX + 1) + ix / (D - 1)] = fabs(cu) + sqrt(g11 * phi);
@@ -1059,28 +1089,28 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         if (r >= tye || c0 >= ncx) continue;
         const int w0 = (r + H) * LX + c0 * (D - 1);
         R *xr = sm + T::XR + r * T::TX + c0 * (D - 1);
-        line_walk2<D, S0X, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, sm + T::LAMX + r * (CX + 1) + c0,
+        line_walk2<D, S0X, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, EigLam{sm + T::CU + r * T::TX + c0 * (D - 1), sm + T::GPX + r * T::TX + c0 * (D - 1), D - 1},
                                  min(S0X, ncx - c0), c0 + S0X >= ncx, xr, xr + T::I, w);
       } else if (it < E0Y) {
         const int j = it - E0X, q = j % T::TX, c0 = (j / T::TX) * S0Y;
         if (q >= txe || c0 >= ncy) continue;
         const int w0 = c0 * (D - 1) * LX + (q + H);
         R *yr = sm + T::YR + q + c0 * (D - 1) * T::TX;
-        line_walk2<D, S0Y, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, sm + T::LAMY + q * (CY + 1) + c0,
+        line_walk2<D, S0Y, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, EigLam{sm + T::CV + c0 * (D - 1) * T::TX + q, sm + T::GPY + c0 * (D - 1) * T::TX + q, (D - 1) * T::TX},
                                       min(S0Y, ncy - c0), c0 + S0Y >= ncy, yr, yr + T::I, w);
       } else if (it < E1X) {
         const int j = it - E0Y, r = j % T::TY, c0 = (j / T::TY) * S1X;
         if (r >= tye || c0 >= ncx) continue;
         const int w0 = (r + H) * LX + c0 * (D - 1);
         R *xr = sm + T::XR + 2 * T::I + r * T::TX + c0 * (D - 1);
-        line_walk<D, S1X, 1, 1, true, R>(sm + T::V + w0, sm + T::V + w0, sm + T::SGNX + r * (CX + 1) + c0,
+        line_walk<D, S1X, 1, 1, true, R>(sm + T::V + w0, sm + T::V + w0, SgnLam{sm + T::CU + r * T::TX + c0 * (D - 1), D - 1},
                                          min(S1X, ncx - c0), c0 + S1X >= ncx, xr, w);
       } else {
         const int j = it - E1X, q = j % T::TX, c0 = (j / T::TX) * S1Y;
         if (q >= txe || c0 >= ncy) continue;
         const int w0 = c0 * (D - 1) * LX + (q + H);
         R *yr = sm + T::YR + 2 * T::I + q + c0 * (D - 1) * T::TX;
-        line_walk<D, S1Y, LX, T::TX, true, R>(sm + T::U + w0, sm + T::U + w0, sm + T::SGNY + q * (CY + 1) + c0,
+        line_walk<D, S1Y, LX, T::TX, true, R>(sm + T::U + w0, sm + T::U + w0, SgnLam{sm + T::CV + c0 * (D - 1) * T::TX + q, (D - 1) * T::TX},
                                               min(S1Y, ncy - c0), c0 + S1Y >= ncy, yr, w);
       }
     }
@@ -1102,10 +1132,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         const bool ends = c0 + nseg == ncx;
         R *xr = sm + T::XR + r * T::TX + c0 * (D - 1);
         if (kk == 0)
-          line_walk2<D, SEGX, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, sm + T::LAMX + r * (CX + 1) + c0, nseg,
+          line_walk2<D, SEGX, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, EigLam{sm + T::CU + r * T::TX + c0 * (D - 1), sm + T::GPX + r * T::TX + c0 * (D - 1), D - 1}, nseg,
                                     ends, xr, xr + T::I, w);
         else
-          line_walk<D, SEGX, 1, 1, true, R>(sm + T::V + w0, sm + T::V + w0, sm + T::SGNX + r * (CX + 1) + c0, nseg,
+          line_walk<D, SEGX, 1, 1, true, R>(sm + T::V + w0, sm + T::V + w0, SgnLam{sm + T::CU + r * T::TX + c0 * (D - 1), D - 1}, nseg,
                                             ends, xr + 2 * T::I, w);
       } else {
         const int j = it - 2 * T::TY * NSX;
@@ -1117,10 +1147,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         const bool ends = c0 + nseg == ncy;
         R *yr = sm + T::YR + q + c0 * (D - 1) * T::TX;
         if (kk == 0)
-          line_walk2<D, SEGY, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, sm + T::LAMY + q * (CY + 1) + c0,
+          line_walk2<D, SEGY, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, EigLam{sm + T::CV + c0 * (D - 1) * T::TX + q, sm + T::GPY + c0 * (D - 1) * T::TX + q, (D - 1) * T::TX},
                                          nseg, ends, yr, yr + T::I, w);
         else
-          line_walk<D, SEGY, LX, T::TX, true, R>(sm + T::U + w0, sm + T::U + w0, sm + T::SGNY + q * (CY + 1) + c0,
+          line_walk<D, SEGY, LX, T::TX, true, R>(sm + T::U + w0, sm + T::U + w0, SgnLam{sm + T::CV + c0 * (D - 1) * T::TX + q, (D - 1) * T::TX},
                                                  nseg, ends, yr + 2 * T::I, w);
       }
     }
@@ -1139,8 +1169,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
       R *xr = sm + T::XR + r * T::TX + c * (D - 1);
       if (kk == 0) {
         float2 d[D];
-        cell_derivs2<D, 1>(d, s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, sm[T::LAMX + r * (CX + 1) + c],
-                           sm[T::LAMX + r * (CX + 1) + c + 1], w);
+        const EigLam lam{sm + T::CU + r * T::TX + c * (D - 1), sm + T::GPX + r * T::TX + c * (D - 1), D - 1};
+        cell_derivs2<D, 1>(d, s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, lam(0), lam(1), w);
 #pragma unroll
         for (int m = 0; m < D; ++m)
           if (m < mmax) {
@@ -1149,8 +1179,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
           }
       } else {
         R d[D];
-        cell_derivs<D, 1, R>(d, sm + T::V + w0, sm + T::V + w0, sm[T::SGNX + r * (CX + 1) + c],
-                             sm[T::SGNX + r * (CX + 1) + c + 1], w);
+        const SgnLam sgn{sm + T::CU + r * T::TX + c * (D - 1), D - 1};
+        cell_derivs<D, 1, R>(d, sm + T::V + w0, sm + T::V + w0, sgn(0), sgn(1), w);
 #pragma unroll
         for (int m = 0; m < D; ++m)
           if (m < mmax) xr[2 * T::I + m] = d[m];
@@ -1167,8 +1197,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
       R *yr = sm + T::YR + (c * (D - 1)) * T::TX + q;
       if (kk == 0) {
         float2 d[D];
-        cell_derivs2<D, LX>(d, s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, sm[T::LAMY + q * (CY + 1) + c],
-                            sm[T::LAMY + q * (CY + 1) + c + 1], w);
+        const EigLam lam{sm + T::CV + c * (D - 1) * T::TX + q, sm + T::GPY + c * (D - 1) * T::TX + q, (D - 1) * T::TX};
+        cell_derivs2<D, LX>(d, s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, lam(0), lam(1), w);
 #pragma unroll
         for (int m = 0; m < D; ++m)
           if (m < mmax) {
@@ -1177,8 +1207,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
           }
       } else {
         R d[D];
-        cell_derivs<D, LX, R>(d, sm + T::U + w0, sm + T::U + w0, sm[T::SGNY + q * (CY + 1) + c],
-                              sm[T::SGNY + q * (CY + 1) + c + 1], w);
+        const SgnLam sgn{sm + T::CV + c * (D - 1) * T::TX + q, (D - 1) * T::TX};
+        cell_derivs<D, LX, R>(d, sm + T::U + w0, sm + T::U + w0, sgn(0), sgn(1), w);
 #pragma unroll
         for (int m = 0; m < D; ++m)
           if (m < mmax) yr[2 * T::I + m * T::TX] = d[m];
@@ -1243,14 +1273,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         const int nseg = min(SEGX, ncx - c0);
         const R *row = sm + (r + H) * LX + c0 * (D - 1);
         R *xr = sm + T::XR + k * T::I + r * T::TX + c0 * (D - 1);
-        const R *lam = sm + T::LAMX + r * (CX + 1) + c0;
+        const ArrLam<R> lam{sm + T::LAMX + r * (CX + 1) + c0};
         const bool ends = c0 + nseg == ncx;
         if (k == 0)
           line_walk<D, SEGX, 1, 1, false, R>(row + T::E, row + T::U, lam, nseg, ends, xr, w);
         else if (k == 1)
           line_walk<D, SEGX, 1, 1, false, R>(row + T::PGU, row + T::PG, lam, nseg, ends, xr, w);
         else
-          line_walk<D, SEGX, 1, 1, true, R>(row + T::V, row + T::V, sm + T::SGNX + r * (CX + 1) + c0, nseg, ends,
+          line_walk<D, SEGX, 1, 1, true, R>(row + T::V, row + T::V, ArrLam<R>{sm + T::SGNX + r * (CX + 1) + c0}, nseg, ends,
                                             xr, w);
       } else {
         const int j = it - 3 * T::TY * NSX;
@@ -1261,14 +1291,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         const int nseg = min(SEGY, ncy - c0);
         const R *col = sm + (q + H) + c0 * (D - 1) * LX;
         R *yr = sm + T::YR + k * T::I + q + c0 * (D - 1) * T::TX;
-        const R *lam = sm + T::LAMY + q * (CY + 1) + c0;
+        const ArrLam<R> lam{sm + T::LAMY + q * (CY + 1) + c0};
         const bool ends = c0 + nseg == ncy;
         if (k == 0)
           line_walk<D, SEGY, LX, T::TX, false, R>(col + T::E, col + T::V, lam, nseg, ends, yr, w);
         else if (k == 1)
           line_walk<D, SEGY, LX, T::TX, false, R>(col + T::PGV, col + T::PG, lam, nseg, ends, yr, w);
         else
-          line_walk<D, SEGY, LX, T::TX, true, R>(col + T::U, col + T::U, sm + T::SGNY + q * (CY + 1) + c0, nseg,
+          line_walk<D, SEGY, LX, T::TX, true, R>(col + T::U, col + T::U, ArrLam<R>{sm + T::SGNY + q * (CY + 1) + c0}, nseg,
                                                  ends, yr, w);
       }
     }
@@ -1528,9 +1558,10 @@ struct StageConfig {
     // carveout shrank L1 and slowed the FP64 kernels by up to 20%)
     cudaError_t e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, 1>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    if (e == cudaSuccess && TMA)
-      e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, kMaxGrids>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    if constexpr (TMA)
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, kMaxGrids>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
     return e;
   }
   static cudaError_t prepare() {
@@ -1546,11 +1577,13 @@ struct StageConfig {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, 1>, NT, SMEM) != cudaSuccess)
       return 0;
-    if (TMA && cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                   &nb, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, kMaxGrids>, NT, SMEM) !=
-                   cudaSuccess)
-      return 0;
-    return TMA ? (nb < n ? nb : n) : n;
+    if constexpr (TMA) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+              &nb, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, kMaxGrids>, NT, SMEM) != cudaSuccess)
+        return 0;
+      return nb < n ? nb : n;
+    }
+    return n;
   }
   static StageLauncher make() {
     static_assert(SMEM <= 227 * 1024, "tile does not fit in shared memory");
