@@ -33,6 +33,18 @@ UNIT = "sim-days/s"
 DEFAULT_HBM_GBS = 6650.0
 
 
+def strict_json(x):
+    """x with every non-finite float replaced by None: the output line stays
+    strict JSON (a forecast that blew up reports null, not NaN)."""
+    if isinstance(x, float):
+        return x if np.isfinite(x) else None
+    if isinstance(x, dict):
+        return {k: strict_json(v) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [strict_json(v) for v in x]
+    return x
+
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -244,7 +256,7 @@ def run_reference(args):
                                        f"(oracle/workloads.py), no GPU library mapped"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "libraries": [m for m in mapped_libraries() if "oracle" in m or "mcv" in m]}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(strict_json(line), allow_nan=False), flush=True)
 
 
 def time_path(args, st, geom, precision, world, barrier, dist, local):
@@ -487,21 +499,26 @@ def run_ours(args):
         twin_phi = st.phi * (1.0 + 1e-12 * np.random.default_rng(0).standard_normal(st.phi.shape))
         runs = {"fp64": ("fp64", st.phi), "fp64_twin": ("fp64", twin_phi), "mixed": ("mixed", st.phi)}
         ncheck = max(1, int(round(args.error_days)))
-        curves, drift = {k: [] for k in runs}, {}
+        curves, drift, finite_days = {k: [] for k in runs}, {}, {}
+        H, n = geom.H, geom.n
         for name, (precision, phi0) in runs.items():
             with api.Stepper(st.order, st.nc, st.dt, st.scheme, precision=precision, radius=6.371e6) as s:
                 s.set_geometry(geom)
                 s.set_member(0, st.phi_s, st.u, st.v, phi0)
                 m0, _ = s.mass_energy(0)
                 done = 0
+                finite_days[name] = 0.0
                 for c in range(ncheck):
                     k = (nsteps * (c + 1)) // ncheck - done
                     s.step(k)
                     done += k
-                    curves[name].append(s.get_state(0)["phi"] / 9.80616)
+                    phi = s.get_state(0)["phi"] / 9.80616
+                    curves[name].append(phi)
+                    if np.isfinite(phi[:, H:H + n, H:H + n]).all() and finite_days[name] == done - k:
+                        finite_days[name] = done
                 m1, _ = s.mass_energy(0)
                 drift[name] = (m1 - m0) / m0
-        H, n = geom.H, geom.n
+                finite_days[name] *= st.dt / 86400.0
 
         def norms(a, b):
             if not np.isfinite(a[:, H:H + n, H:H + n]).all():
@@ -517,6 +534,8 @@ def run_ours(args):
                     "curve_days": days, "mixed_L2_curve": [c[1] for c in mixed_curve],
                     "fp64_twin_L2_curve": [c[1] for c in twin_curve],
                     "mass_drift": {"fp64": drift["fp64"], "mixed": drift["mixed"]},
+                    # the last check (in simulated days) up to which each run stayed finite
+                    "finite_through_days": finite_days,
                     "reference": "FP64 GPU path (oracle-validated by the parity tests); fp64_twin: the FP64 "
                                  "path from phi*(1+1e-12*N(0,1))"}
 
@@ -554,7 +573,7 @@ def run_ours(args):
                 "fp64_gpu_vs_cpu_baseline": (paths["fp64"]["value"] / cpu["value"]
                                              if cpu and "fp64" in paths else None),
                 "accuracy": accuracy, **extra}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(strict_json(line), allow_nan=False), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

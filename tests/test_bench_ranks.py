@@ -44,3 +44,16 @@ def test_two_ranks_take_the_slowest_time():
         assert res[r][3] == pytest.approx(15.0)
         # 2 replicas x 100 steps x 30 s in 15 ms of job time
         assert res[r][4] == pytest.approx(2 * 100 * 30.0 / 86400.0 / 0.015)
+
+
+def test_output_line_is_strict_json():
+    """A forecast that went non-finite reports null: the line stays strict JSON."""
+    import json
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    line = {"value": 1.5, "accuracy": {"L2": float("nan"), "curve": [1e-8, np.float64("inf"), -np.inf],
+                                       "drift": (np.float64(2.0), np.nan)}, "n": 3, "s": "x"}
+    out = json.loads(json.dumps(bench.strict_json(line), allow_nan=False))
+    assert out == {"value": 1.5, "accuracy": {"L2": None, "curve": [1e-8, None, None], "drift": [2.0, None]},
+                   "n": 3, "s": "x"}
