@@ -384,9 +384,10 @@ void launch_halo_batch(mcv_handle *const *hs, const int *curs, int count, int s,
   b.first[count] = slots;
   b.ngrids = count;
   const bool mixed_inc = hs[0]->mixed && !last_stage(stage_kind(hs[0], s));
-  const int block = 128;
-  // x: positions along an edge; y: 4 edges x 6 panels x (H+1) lines; z: grids' active members
-  const dim3 grid((unsigned)((nmax + block - 1) / block), (unsigned)(24 * (hs[0]->H + 1)), (unsigned)slots);
+  // x: segments of kHaloSeg positions along an edge; y: 6 panels x 4 edges;
+  // z: grids' active members.  A block holds the segment's H + 1 lines.
+  const int block = kHaloSeg * (hs[0]->H + 1);
+  const dim3 grid((unsigned)((nmax + kHaloSeg - 1) / kHaloSeg), 24u, (unsigned)slots);
   if (hs[0]->order == 3) {
     if (mixed_inc) halo_kernel<3, true, NB><<<grid, block, 0, st>>>(b);
     else halo_kernel<3, false, NB><<<grid, block, 0, st>>>(b);

@@ -88,19 +88,35 @@ struct HaloBatch {
   int ngrids;
 };
 
+// Positions along an edge per block, and the window of neighbour positions a
+// block stages per halo line: the ghost points of kHaloSeg consecutive
+// positions reference at most kHaloSeg + 3 consecutive points of the
+// neighbour's line (ghost%iref is monotone along an edge; 67 for 64 at every
+// Nc of the equiangular grids), and a reference outside the window is read
+// from global memory instead.
+constexpr int kHaloSeg = 64, kHaloWin = 72;
+
 // MIXED: the field completed is Y + increment.  Raw values combine Y with the
 // increment in FP64; the result minus Y at the destination is stored as the
 // new FP32 increment, so the next stage's input halo is the FP64 correction
 // of its own interior.
+//
+// One block per (segment of kHaloSeg positions: x; panel and edge: y; grid and
+// active member: z), one thread per (position, line h = 0..H), positions
+// fastest so that a warp shares its line.  The block first stages the
+// neighbour's lines 1..H over the segment's window -- each point loaded once,
+// completed and rotated to the sphere once, with the loads coalesced along
+// the neighbour's rows (lines fastest on a W/E neighbour edge, whose lines are
+// columns) -- then interpolates the ghost points from shared memory.
 template <int D, bool MIXED, int NB>
-__global__ void __launch_bounds__(128) halo_kernel(const __grid_constant__ HaloBatch<NB> hb) {
+__global__ void __launch_bounds__(kHaloSeg * D) halo_kernel(const __grid_constant__ HaloBatch<NB> hb) {
   constexpr int H = D - 1;
+  constexpr int NT = kHaloSeg * (H + 1);
   // the next stage kernel may launch now: its items clear of the panel edges
   // read nothing this kernel writes, the others wait for its completion
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  // one thread per (position k along the edge: x; panel, edge and halo line
-  // h = 0..H: y; grid and active member: z) -- no runtime divisions before
-  // the first loads
+  // the staged neighbour lines 1..H: {zonal, meridional, phi} on the sphere
+  __shared__ double wz[H][kHaloWin], wm[H][kHaloWin], wp[H][kHaloWin];
   const int z = blockIdx.z;
   int kg = 0;
 #pragma unroll
@@ -109,17 +125,18 @@ __global__ void __launch_bounds__(128) halo_kernel(const __grid_constant__ HaloB
   const GridDesc &g = hb.g[kg];
   const HaloArgs &a = hb.a[kg];
   const int n = g.n;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+  const int k0 = blockIdx.x * kHaloSeg;
+  if (k0 >= n) return;  // block-uniform: the grid is sized for the batch's largest grid
   const int slot = z - hb.first[kg];
   const int mem = __ldg(a.active + slot);
-  const int h = blockIdx.y % (H + 1);
-  const int pe = blockIdx.y / (H + 1);
-  const int p = pe >> 2, e = pe & 3;
+  const int p = blockIdx.y >> 2, e = blockIdx.y & 3;
   const EdgeLink L = c_links[p][e];
   const int q = L.q, e2 = L.e2;
   const long long mb = (long long)mem * g.mstride;
   const long long bb = (long long)mem * 24 * n;
+  const int h = threadIdx.x / kHaloSeg;      // this thread's line
+  const int k = k0 + threadIdx.x % kHaloSeg;  // and position
+  const bool live = k < n;
 
   // raw (pre-unification) value of boundary point (i, j) of panel pp
   auto raw_boundary = [&](int pp, int i, int j, double &su, double &sv, double &sp) {
@@ -133,115 +150,141 @@ __global__ void __launch_bounds__(128) halo_kernel(const __grid_constant__ HaloB
       su = a.u[o] + (double)b.x; sv = a.v[o] + (double)b.y; sp = a.phi[o] + (double)b.z;
     }
   };
+  // the completed field at position kk of the neighbour's line hh (1..H),
+  // rotated to the sphere (covProjPlane2Sphere, projection_mod.F90:79-96).  A
+  // point at an end of the line is a boundary point and takes its raw copy;
+  // the FP64 form, whose boundary this kernel rewrites, reads no state there.
+  auto neighbour = [&](int hh, int kk, double &zq, double &mq, double &pq) {
+    const int ks = L.rev ? n - 1 - kk : kk;
+    const bool isb = (ks == 0 || ks == n - 1);
+    int si, sj;
+    strip_point(e2, hh, ks, n, si, sj);
+    const double4 M = a.Mtab[((q * 4 + e2) * (H + 1) + hh) * n + ks];
+    double su, sv, sp;
+    if constexpr (MIXED) {
+      const long long os = mb + q * g.plane + (long long)(sj + H) * g.P + (si + H);
+      const double yu = a.u[os], yv = a.v[os], yp = a.phi[os];
+      float du, dv, dp;
+      if (isb) {
+        const float4 b = a.bnd32[bb + q * 4 * n + boundary_slot(si, sj, n)];
+        du = b.x; dv = b.y; dp = b.z;
+      } else {
+        du = a.du[os]; dv = a.dv[os]; dp = a.dp[os];
+      }
+      su = yu + (double)du;
+      sv = yv + (double)dv;
+      sp = yp + (double)dp;
+    } else if (isb) {
+      const double4 b = a.bnd[bb + q * 4 * n + boundary_slot(si, sj, n)];
+      su = b.x; sv = b.y; sp = b.z;
+    } else {
+      const long long os = mb + q * g.plane + (long long)(sj + H) * g.P + (si + H);
+      su = a.u[os]; sv = a.v[os]; sp = a.phi[os];
+    }
+    zq = M.x * su + M.z * sv;
+    mq = M.y * su + M.w * sv;
+    pq = sp;
+  };
 
-  // destination point and its rotation, loaded ahead of the dependent loads
-  int di, dj;
-  strip_point(e, -h, k, n, di, dj);
-  const long long o = mb + p * g.plane + (long long)(dj + H) * g.P + (di + H);
-  const double4 N = a.Ntab[((p * 4 + e) * (H + 1) + h) * n + k];
+  // this thread's destination, its rotation back and (split precision) the Y
+  // it corrects; the interpolation weights of a ghost line
+  int di = 0, dj = 0;
+  long long o = 0;
+  double4 N{};
   double yu_d = 0., yv_d = 0., yp_d = 0.;
-  if constexpr (MIXED) {
-    yu_d = a.u[o];
-    yv_d = a.v[o];
-    yp_d = a.phi[o];
+  int iref = 1;
+  double2 cc{};
+  if (live) {
+    strip_point(e, -h, k, n, di, dj);
+    o = mb + p * g.plane + (long long)(dj + H) * g.P + (di + H);
+    N = a.Ntab[((p * 4 + e) * (H + 1) + h) * n + k];
+    if constexpr (MIXED) {
+      yu_d = a.u[o];
+      yv_d = a.v[o];
+      yp_d = a.phi[o];
+    }
+    if (h > 0) {
+      iref = a.giref[(h - 1) * n + k];
+      cc = a.gcoef[(h - 1) * n + k];
+    }
   }
 
-  double zw, mw, ph;
-  if (h > 0) {
-    // halo line h: neighbour line h rotated to the sphere, interpolated along
-    // the edge, rotated back to this panel (ghost_mod.f90:154-181).  The D
-    // neighbour points' loads are all issued before any is used: a point at an
-    // end of the line is a boundary point and takes its raw copy; the state
-    // load of such a point goes to its inner neighbour instead (FP64 form: the
-    // boundary itself is rewritten by this kernel) and is not used.
-    const int iref = a.giref[(h - 1) * n + k];
-    const double2 cc = a.gcoef[(h - 1) * n + k];
-    double yu[D], yv[D], yp[D];
-    double4 M[D], bv[D];
-    float4 b32[D];
-    float du[D], dv[D], dp[D];
-    bool isb[D];
+  // the boundary line (h = 0) needs no staged values
+  bool store = live;
+  double zw = 0., mw = 0., ph = 0.;
+  if (live && h == 0) {
+    if (k > 0 && k < n - 1) {
+      // edge average (spatial_operators_mod.F90:298-345)
+      const int ks = L.rev ? n - 1 - k : k;
+      int oi, oj, ni, nj;
+      strip_point(e, 0, k, n, oi, oj);
+      strip_point(e2, 0, ks, n, ni, nj);
+      double ou, ov, op, nu, nv, np_;
+      raw_boundary(p, oi, oj, ou, ov, op);
+      raw_boundary(q, ni, nj, nu, nv, np_);
+      const double4 Mo = a.Mtab[((p * 4 + e) * (H + 1) + 0) * n + k];
+      const double4 Mn = a.Mtab[((q * 4 + e2) * (H + 1) + 0) * n + ks];
+      zw = 0.5 * ((Mo.x * ou + Mo.z * ov) + (Mn.x * nu + Mn.z * nv));
+      mw = 0.5 * ((Mo.y * ou + Mo.w * ov) + (Mn.y * nu + Mn.w * nv));
+      ph = 0.5 * (op + np_);
+    } else if (e <= 1) {
+      // cube vertex (:347-386), owned by the W/E edge threads
+      const int corner = (e == 0) ? (k == 0 ? 0 : 2) : (k == 0 ? 1 : 3);
+      const VertexRef V = c_vertex[p][corner];
+      double zz[3], mm[3], pp[3];
 #pragma unroll
-    for (int m = 0; m < D; ++m) {
-      const int kk = (iref - 1) * (D - 1) + m;
-      const int ks = L.rev ? n - 1 - kk : kk;
-      isb[m] = (ks == 0 || ks == n - 1);
-      int si, sj;
-      strip_point(e2, h, ks, n, si, sj);
-      const int bslot = boundary_slot(si, sj, n);
-      const int kc = MIXED ? ks : min(max(ks, 1), n - 2);
-      strip_point(e2, h, kc, n, si, sj);
-      const long long os = mb + q * g.plane + (long long)(sj + H) * g.P + (si + H);
-      yu[m] = a.u[os];
-      yv[m] = a.v[os];
-      yp[m] = a.phi[os];
-      if constexpr (MIXED) {
-        b32[m] = a.bnd32[bb + q * 4 * n + bslot];
-        du[m] = a.du[os];
-        dv[m] = a.dv[os];
-        dp[m] = a.dp[os];
-      } else {
-        bv[m] = a.bnd[bb + q * 4 * n + bslot];
+      for (int t = 0; t < 3; ++t) {
+        const int pt = V.panel[t], ct = V.corner[t];
+        const int et = (ct == 0 || ct == 2) ? 0 : 1;  // W or E column holds the corner
+        const int kt = (ct <= 1) ? 0 : n - 1;
+        double bu, bv, bp;
+        raw_boundary(pt, et == 0 ? 0 : n - 1, kt, bu, bv, bp);
+        const double4 M = a.Mtab[((pt * 4 + et) * (H + 1) + 0) * n + kt];
+        zz[t] = M.x * bu + M.z * bv;
+        mm[t] = M.y * bu + M.w * bv;
+        pp[t] = bp;
       }
-      M[m] = a.Mtab[((q * 4 + e2) * (H + 1) + h) * n + ks];
+      zw = (zz[0] + zz[1] + zz[2]) / 3.;
+      mw = (mm[0] + mm[1] + mm[2]) / 3.;
+      ph = (pp[0] + pp[1] + pp[2]) / 3.;
+    } else {
+      store = false;  // an S/N edge's end: the vertex, written by the W/E threads
     }
+  }
+
+  // stage the neighbour's lines 1..H over the window [lo, lo + kHaloWin) of
+  // each line, lo = the first point the segment's first ghost point uses
+  auto window_lo = [&](int hh) { return (a.giref[(hh - 1) * n + k0] - 1) * (D - 1); };
+  for (int s = threadIdx.x; s < H * kHaloWin; s += NT) {
+    const int hh = (e2 <= 1) ? 1 + s % H : 1 + s / kHaloWin;
+    const int t = (e2 <= 1) ? s / H : s % kHaloWin;
+    const int kk = window_lo(hh) + t;
+    if (kk <= n - 1) neighbour(hh, kk, wz[hh - 1][t], wm[hh - 1][t], wp[hh - 1][t]);
+  }
+  __syncthreads();
+
+  if (live && h > 0) {
+    // halo line h: the neighbour's line h on the sphere, interpolated along
+    // the edge (ghost_mod.f90:154-181)
+    const int lo = window_lo(h);
     double qz[D], qm[D], qp[D];
 #pragma unroll
     for (int m = 0; m < D; ++m) {
-      double su, sv, sp;
-      if constexpr (MIXED) {
-        su = yu[m] + (double)(isb[m] ? b32[m].x : du[m]);
-        sv = yv[m] + (double)(isb[m] ? b32[m].y : dv[m]);
-        sp = yp[m] + (double)(isb[m] ? b32[m].z : dp[m]);
+      const int kk = (iref - 1) * (D - 1) + m;
+      const int t = kk - lo;
+      if (t >= 0 && t < kHaloWin) {
+        qz[m] = wz[h - 1][t];
+        qm[m] = wm[h - 1][t];
+        qp[m] = wp[h - 1][t];
       } else {
-        su = isb[m] ? bv[m].x : yu[m];
-        sv = isb[m] ? bv[m].y : yv[m];
-        sp = isb[m] ? bv[m].z : yp[m];
+        neighbour(h, kk, qz[m], qm[m], qp[m]);
       }
-      qz[m] = M[m].x * su + M[m].z * sv;  // covProjPlane2Sphere, projection_mod.F90:79-96
-      qm[m] = M[m].y * su + M[m].w * sv;
-      qp[m] = sp;
     }
     zw = ghost_interp<D>(qz, cc.x, cc.y, a);
     mw = ghost_interp<D>(qm, cc.x, cc.y, a);
     ph = ghost_interp<D>(qp, cc.x, cc.y, a);
-  } else if (k > 0 && k < n - 1) {
-    // boundary line: edge average (spatial_operators_mod.F90:298-345)
-    const int ks = L.rev ? n - 1 - k : k;
-    int oi, oj, ni, nj;
-    strip_point(e, 0, k, n, oi, oj);
-    strip_point(e2, 0, ks, n, ni, nj);
-    double ou, ov, op, nu, nv, np_;
-    raw_boundary(p, oi, oj, ou, ov, op);
-    raw_boundary(q, ni, nj, nu, nv, np_);
-    const double4 Mo = a.Mtab[((p * 4 + e) * (H + 1) + 0) * n + k];
-    const double4 Mn = a.Mtab[((q * 4 + e2) * (H + 1) + 0) * n + ks];
-    zw = 0.5 * ((Mo.x * ou + Mo.z * ov) + (Mn.x * nu + Mn.z * nv));
-    mw = 0.5 * ((Mo.y * ou + Mo.w * ov) + (Mn.y * nu + Mn.w * nv));
-    ph = 0.5 * (op + np_);
-  } else if (e <= 1) {
-    // cube vertex (:347-386), owned by the W/E edge threads
-    const int corner = (e == 0) ? (k == 0 ? 0 : 2) : (k == 0 ? 1 : 3);
-    const VertexRef V = c_vertex[p][corner];
-    double z[3], mm[3], pp[3];
-#pragma unroll
-    for (int t = 0; t < 3; ++t) {
-      const int pt = V.panel[t], ct = V.corner[t];
-      const int et = (ct == 0 || ct == 2) ? 0 : 1;  // W or E column holds the corner
-      const int kt = (ct <= 1) ? 0 : n - 1;
-      double bu, bv, bp;
-      raw_boundary(pt, et == 0 ? 0 : n - 1, kt, bu, bv, bp);
-      const double4 M = a.Mtab[((pt * 4 + et) * (H + 1) + 0) * n + kt];
-      z[t] = M.x * bu + M.z * bv;
-      mm[t] = M.y * bu + M.w * bv;
-      pp[t] = bp;
-    }
-    zw = (z[0] + z[1] + z[2]) / 3.;
-    mw = (mm[0] + mm[1] + mm[2]) / 3.;
-    ph = (pp[0] + pp[1] + pp[2]) / 3.;
-  } else {
-    return;
   }
+  if (!store) return;
   // back to this panel's covariant winds (covProjSphere2Plane, :459-492)
   const double uo = N.x * zw + N.z * mw, vo = N.y * zw + N.w * mw;
   if constexpr (!MIXED) {
