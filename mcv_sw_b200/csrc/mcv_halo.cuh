@@ -89,12 +89,13 @@ struct HaloBatch {
 };
 
 // Positions along an edge per block, and the window of neighbour positions a
-// block stages per halo line: the ghost points of kHaloSeg consecutive
-// positions reference at most kHaloSeg + 3 consecutive points of the
-// neighbour's line (ghost%iref is monotone along an edge; 67 for 64 at every
-// Nc of the equiangular grids), and a reference outside the window is read
-// from global memory instead.
-constexpr int kHaloSeg = 64, kHaloWin = 72;
+// block stages per halo line.  The interpolation stencil of the ghost point at
+// position k starts at neighbour position (iref - 1)(D - 1), within [k - 6,
+// k + 2] on every line at every Nc of the equiangular grids, so the window
+// [k0 - kHaloLead, k0 - kHaloLead + kHaloWin) of a segment starting at k0
+// holds all of its stencils without reading iref first; a stencil point
+// outside the window is read from global memory instead.
+constexpr int kHaloSeg = 64, kHaloLead = 8, kHaloWin = kHaloSeg + 16;
 
 // MIXED: the field completed is Y + increment.  Raw values combine Y with the
 // increment in FP64; the result minus Y at the destination is stored as the
@@ -252,13 +253,12 @@ __global__ void __launch_bounds__(kHaloSeg * D) halo_kernel(const __grid_constan
     }
   }
 
-  // stage the neighbour's lines 1..H over the window [lo, lo + kHaloWin) of
-  // each line, lo = the first point the segment's first ghost point uses
-  auto window_lo = [&](int hh) { return (a.giref[(hh - 1) * n + k0] - 1) * (D - 1); };
+  // stage the neighbour's lines 1..H over the window [lo, lo + kHaloWin)
+  const int lo = max(k0 - kHaloLead, 0);
   for (int s = threadIdx.x; s < H * kHaloWin; s += NT) {
     const int hh = (e2 <= 1) ? 1 + s % H : 1 + s / kHaloWin;
     const int t = (e2 <= 1) ? s / H : s % kHaloWin;
-    const int kk = window_lo(hh) + t;
+    const int kk = lo + t;
     if (kk <= n - 1) neighbour(hh, kk, wz[hh - 1][t], wm[hh - 1][t], wp[hh - 1][t]);
   }
   __syncthreads();
@@ -266,7 +266,6 @@ __global__ void __launch_bounds__(kHaloSeg * D) halo_kernel(const __grid_constan
   if (live && h > 0) {
     // halo line h: the neighbour's line h on the sphere, interpolated along
     // the edge (ghost_mod.f90:154-181)
-    const int lo = window_lo(h);
     double qz[D], qm[D], qp[D];
 #pragma unroll
     for (int m = 0; m < D; ++m) {
