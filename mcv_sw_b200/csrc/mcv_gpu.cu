@@ -140,6 +140,9 @@ struct mcv_handle {
   int *active = nullptr;
   std::vector<int> active_host;
   int n_active = 0;
+  // active_host[k] == k for every k: the kernels take the slot as the member
+  // index without reading the list (the step graphs bake this in)
+  bool active_ident = true;
   int *flags = nullptr;  // non-finite flags [members]
   int *err = nullptr;    // stage-kernel error flag (TMA staging timed out)
   double *stage = nullptr;  // one FP64 field in the host's dense layout (PCIe copies land here)
@@ -285,6 +288,7 @@ StageArgs stage_args(mcv_handle *h, int s, int c) {
   a.phis = h->phis;
   a.bnd = h->bnd;
   a.active = h->active;
+  a.ident = h->active_ident ? 1 : 0;
   a.err = h->err;
   const double dt = h->dt;
   const int kind = stage_kind(h, s);
@@ -347,6 +351,7 @@ HaloArgs halo_args(mcv_handle *h, int s, int c) {
   a.r2dx3 = 1. / (2. * h->dx3);
   a.members = h->n_active;
   a.active = h->active;
+  a.ident = h->active_ident ? 1 : 0;
   const int kind = stage_kind(h, s);
   if (!h->mixed) {
     double *const *out = (kind == RK3_S1 || kind == RK4_S1 || kind == RK4_S3) ? h->A
@@ -498,12 +503,13 @@ int launch_stage(mcv_handle *h, int cand, int s, int c) {
   if (int rc = add_grid(b, 0, h, L, s, c)) return rc;
   number_items(b, 1);
   const int kind = stage_kind(h, s);
+  const StageLaunchFn launch = h->active_ident ? L.launch_ident[kind] : L.launch[kind];
   if (!L.tma) {
-    L.launch[kind](dim3(b.g[0].tiles_x * b.g[0].tiles_y, 6, h->n_active), h->stream, b);
+    launch(dim3(b.g[0].tiles_x * b.g[0].tiles_y, 6, h->n_active), h->stream, b);
     return MCV_OK;
   }
   const int ctas = std::max(1, std::min(b.total, h->bps[cand] * h->nsm));
-  L.launch[kind](dim3(ctas), h->stream, b);
+  launch(dim3(ctas), h->stream, b);
   return MCV_OK;
 }
 
@@ -763,6 +769,7 @@ extern "C" int mcv_create(int order, int nc, int scheme, int precision, double d
   h->active_host.resize(members);
   for (int m = 0; m < members; ++m) h->active_host[m] = m;
   h->n_active = members;
+  h->active_ident = true;
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(h->active, h->active_host.data(), sizeof(int) * members, cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -1220,8 +1227,11 @@ extern "C" int mcv_set_active(mcv_handle *h, int count, const int *members) {
     if (seen[m]) return fail(MCV_ERR_ARG, "active member listed twice");
     seen[m] = 1;
   }
-  if (count != h->n_active) {
-    // the step graphs hold the launch grids: rebuild before the next step
+  bool ident = true;
+  for (int k = 0; k < count; ++k) ident = ident && members[k] == k;
+  if (count != h->n_active || ident != h->active_ident) {
+    // the step graphs hold the launch grids and whether the list is the
+    // identity: rebuild before the next step
     MCV_CUDA(cudaStreamSynchronize(h->stream), "drain before changing the active set");
     for (int c = 0; c < 2; ++c)
       if (h->graph_exec[c]) {
@@ -1245,6 +1255,7 @@ extern "C" int mcv_set_active(mcv_handle *h, int count, const int *members) {
     }
   }
   h->n_active = count;
+  h->active_ident = ident;
   // ordered after the steps already enqueued on the handle's stream; a copy
   // from pageable memory has consumed the host list when it returns
   if (count > 0)
@@ -1578,10 +1589,11 @@ struct mcv_group {
   cudaEvent_t done = nullptr;
   std::vector<cudaEvent_t> ready;  // per handle: work queued on its own stream before a group step
   // step graphs: built for the members' buffer parities `key_cur` (and their
-  // complement, which the next step has) and active counts `key_active`
+  // complement, which the next step has), active counts `key_active` and
+  // whether each active list is the identity `key_ident`
   cudaGraphExec_t graph[2]{};
   std::vector<mcv_handle *> key_hs;  // the handles with active members the graphs advance
-  std::vector<int> key_cur, key_active;
+  std::vector<int> key_cur, key_active, key_ident;
 };
 
 namespace {
@@ -1635,17 +1647,19 @@ int build_group_graphs(mcv_group *g, const std::vector<mcv_handle *> &act) {
   g->key_hs = act;
   g->key_cur.resize(act.size());
   g->key_active.resize(act.size());
+  g->key_ident.resize(act.size());
   for (size_t k = 0; k < act.size(); ++k) {
     g->key_cur[k] = act[k]->mixed ? act[k]->cur : 0;
     g->key_active[k] = act[k]->n_active;
+    g->key_ident[k] = act[k]->active_ident;
   }
   return MCV_OK;
 }
 
 // The handles a group step advances (those with active members) and the step
 // graph to replay first (0, or 1 when the parities are one step on), rebuilt
-// unless the handles, active counts and buffer parities are the ones the
-// graphs were built for.
+// unless the handles, active counts, identity of the active lists and buffer
+// parities are the ones the graphs were built for.
 int prepare_group(mcv_group *g, std::vector<mcv_handle *> &act, int &flip) {
   act.clear();
   for (mcv_handle *h : g->hs) {
@@ -1660,7 +1674,7 @@ int prepare_group(mcv_group *g, std::vector<mcv_handle *> &act, int &flip) {
     int eq = 1, cp = 1;
     for (size_t k = 0; k < act.size(); ++k) {
       const int c = act[k]->mixed ? act[k]->cur : 0;
-      same = same && g->key_active[k] == act[k]->n_active;
+      same = same && g->key_active[k] == act[k]->n_active && g->key_ident[k] == (int)act[k]->active_ident;
       eq = eq && c == g->key_cur[k];
       cp = cp && c == 1 - g->key_cur[k];
     }

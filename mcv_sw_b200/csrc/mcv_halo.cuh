@@ -16,6 +16,7 @@ struct HaloArgs {
   double rdx, rdx2, r2dx3;    // 1/dx, 1/dx**2., 1/(2 dx**3.)
   int members;                // active members in this launch
   const int *active;          // member index of each active slot [members]
+  int ident;                  // 1 when active[k] == k for every slot: the slot is the member
   // split precision: the field completed is Y + increment; u/v/phi above are
   // Y (read only), the increment's halo and boundary are written instead
   float *du, *dv, *dp;
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(kHaloSeg * D) halo_kernel(const __grid_constan
   const int k0 = blockIdx.x * kHaloSeg;
   if (k0 >= n) return;  // block-uniform: the grid is sized for the batch's largest grid
   const int slot = z - hb.first[kg];
-  const int mem = __ldg(a.active + slot);
+  const int mem = active_member(a.active, a.ident, slot);
   const int p = blockIdx.y >> 2, e = blockIdx.y & 3;
   const EdgeLink L = c_links[p][e];
   const int q = L.q, e2 = L.e2;

@@ -65,6 +65,7 @@ struct StageArgs {
   double inc;    // dt or dt/2 (update_stat's inc_t) or the RK3 tendency weight
   int *err;      // set to 1 if a staged tile's copies did not arrive in time (TMA form)
   const int *active;  // member index of each grid z slice (the members this launch advances)
+  int ident;          // 1 when active[k] == k for every slot: the slot is the member, no load
   // ---- split-precision policy ----
   const double *yu, *yv, *yp;  // FP64 state Y (RK base and stage-1 input), padded; the last
                                // stage writes Y + increment to uo/vo/po (the other state buffer)
@@ -582,6 +583,15 @@ __device__ __forceinline__ WorkItem decode_batch(const StageBatch<NB> &b, int wi
 
 // PTX programmatic dependent launch: wait until the preceding kernel (the halo
 // kernel) has completed and its writes are visible; let the next kernel launch.
+// The member an active slot advances.  With an identity list (ident) it is the
+// slot itself; the load sits in inline assembly so that it is not hoisted
+// above the test and waited for on the identity path.
+__device__ __forceinline__ int active_member(const int *active, int ident, int slot) {
+  if (ident) return slot;
+  int m;
+  asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(m) : "l"(active + slot));
+  return m;
+}
 __device__ __forceinline__ void wait_prerequisite_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
@@ -600,7 +610,11 @@ __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddep
 // linear references in the step's first stage and stores them, and the later
 // stages' copies bring them in with the tile.  Otherwise one CTA per (tile,
 // panel, member) loads its fields with ordinary loads.
-template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA, int OPT, int NB>
+// IDENT: a one-grid launch whose active list is the identity (the member of a
+// slot is the slot, known to the compiler); otherwise the list is read, or
+// skipped at run time when StageArgs::ident says it is the identity.
+template <int D, int CX, int CY, int NT, int MINB, int KIND, bool MIXED, int WALK, bool TMA, int OPT, int NB,
+          bool IDENT = false>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__ StageBatch<NB> b) {
   using R = std::conditional_t<MIXED, float, double>;
   using T = Tile<D, CX, CY, R>;
@@ -640,7 +654,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
       wait_prerequisite_grid();
       waited = true;
     }
-    const int panel = it.panel, mem = __ldg(a.active + it.slot);
+    const int panel = it.panel, mem = IDENT ? it.slot : active_member(a.active, a.ident, it.slot);
     const int X0 = it.tx * CX * (D - 1), Y0 = it.ty * CY * (D - 1);
     uint32_t bytes = 0;
 #pragma unroll
@@ -702,14 +716,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
     tx = item.tx;
     ty = item.ty;
     panel = item.panel;
-    mem = __ldg(a.active + item.slot);
+    mem = IDENT ? item.slot : active_member(a.active, a.ident, item.slot);
   } else {
     // one CTA per (tile, panel, member) in panel order, which keeps the
     // neighbours' halo reads in L2; it starts once the previous kernel is done
     tx = blockIdx.x % g.tiles_x;
     ty = blockIdx.x / g.tiles_x;
     panel = blockIdx.y;
-    mem = __ldg(a.active + blockIdx.z);
+    mem = IDENT ? (int)blockIdx.z : active_member(a.active, a.ident, (int)blockIdx.z);
     wait_prerequisite_grid();
   }
   const int c0x = tx * CX, c0y = ty * CY;
@@ -1515,6 +1529,7 @@ struct StageLauncher {
   size_t smem;
   int box_x, box_y;              // staged box of one field (TMA form)
   StageLaunchFn launch[7];       // one grid, indexed by StageKind
+  StageLaunchFn launch_ident[7]; // one grid whose active list is the identity
   StageBatchFn launch_batch[7];  // up to kMaxGrids grids in one launch (TMA form; else null)
   cudaError_t (*prepare)();      // raises the dynamic shared-memory limit of every kind
   int (*blocks_per_sm)();        // resident CTAs per SM (sizes the persistent grid)
@@ -1530,7 +1545,7 @@ struct StageConfig {
   // launched with programmatic stream serialization: the kernel's CTAs may
   // become resident while the preceding halo kernel finishes (TMA form: items
   // clear of the panel edges also run then; the rest wait for it)
-  template <int KIND, int NB>
+  template <int KIND, int NB, bool IDENT = false>
   static void launch_nb(dim3 grid, cudaStream_t s, const StageBatch<NB> &b) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
@@ -1542,11 +1557,15 @@ struct StageConfig {
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, NB>, b);
+    cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, NB, IDENT>, b);
   }
   template <int KIND>
   static void launch(dim3 grid, cudaStream_t s, const StageBatch<1> &b) {
     launch_nb<KIND, 1>(grid, s, b);
+  }
+  template <int KIND>
+  static void launch_ident(dim3 grid, cudaStream_t s, const StageBatch<1> &b) {
+    launch_nb<KIND, 1, true>(grid, s, b);
   }
   template <int KIND>
   static void launch_batch(dim3 grid, cudaStream_t s, const StageBatch<kMaxGrids> &b) {
@@ -1558,6 +1577,9 @@ struct StageConfig {
     // carveout shrank L1 and slowed the FP64 kernels by up to 20%)
     cudaError_t e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, 1>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, 1, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
     if constexpr (TMA)
       if (e == cudaSuccess)
         e = cudaFuncSetAttribute(stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, kMaxGrids>,
@@ -1571,12 +1593,15 @@ struct StageConfig {
       return e;
     return cudaSuccess;
   }
-  // resident CTAs per SM (the smaller of the one-grid and the batched forms)
+  // resident CTAs per SM (the smallest over the one-grid and the batched forms)
   static int blocks_per_sm() {
-    int n = 0, nb = 0;
+    int n = 0, ni = 0, nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, 1>, NT, SMEM) != cudaSuccess)
+            &n, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, 1>, NT, SMEM) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &ni, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, 1, true>, NT, SMEM) != cudaSuccess)
       return 0;
+    if (ni < n) n = ni;
     if constexpr (TMA) {
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
               &nb, stage_kernel<D, CX, CY, NT, MINB, 1, MIXED, WALK, TMA, OPT, kMaxGrids>, NT, SMEM) != cudaSuccess)
@@ -1590,6 +1615,8 @@ struct StageConfig {
     static_assert(MINB * (SMEM + 1024) <= 228 * 1024, "MINB tiles do not fit in one SM's shared memory");
     StageLauncher L{CX, CY, NT, MINB, WALK, TMA, SMEM, T::BX, T::LY,
                     {&launch<0>, &launch<1>, &launch<2>, &launch<3>, &launch<4>, &launch<5>, &launch<6>},
+                    {&launch_ident<0>, &launch_ident<1>, &launch_ident<2>, &launch_ident<3>, &launch_ident<4>,
+                     &launch_ident<5>, &launch_ident<6>},
                     {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr}, &prepare, &blocks_per_sm};
     if constexpr (TMA) {
       StageBatchFn fb[7] = {&launch_batch<0>, &launch_batch<1>, &launch_batch<2>, &launch_batch<3>,
