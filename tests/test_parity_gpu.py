@@ -138,6 +138,39 @@ def test_every_tile_shape_agrees(order):
             assert d < TILE_TOL, (i, k, d)
 
 
+@pytest.mark.parametrize("order,nc,members", [(4, 96, 1), (3, 64, 2)])
+def test_every_persistent_shape_over_many_items(order, nc, members):
+    """The TMA-staged persistent shapes walk several work items per CTA here
+    (MCV4 Nc=96: 864 items; MCV3 Nc=64, two members: 1,536), so the staging
+    buffer and its mbarrier phase cycle: every such FP64 shape stays within TOL
+    of the oracle after 3 RK4 steps, for an identity active list and for a
+    permuted one."""
+    nsteps = 3
+    geom = api.Geometry(order, nc, cases.EARTH_RADIUS)
+    st = cases.finish(geom, *cases.balanced_flow(geom, np.random.default_rng(17), mountain=True)[:4], "RK4",
+                      nsteps=nsteps)
+    o = oracle_for(st)
+    o.step(nsteps)
+    with api.Stepper(order, nc, st.dt, "RK4", members=members) as s:
+        s.set_geometry(geom)
+        for m in range(members):
+            s.set_member(m, st.phi_s, st.u, st.v, st.phi)
+        cands, _ = s.tuning()  # runs the autotuner, which needs the members
+        persistent = [i for i, (shape, _) in enumerate(cands) if shape[5] == 1]
+        assert persistent
+        for i in persistent:
+            for active in ([*range(members)], [*range(members)][::-1]):
+                s.select_tile(i)
+                for m in range(members):
+                    s.set_member(m, st.phi_s, st.u, st.v, st.phi)
+                s.set_active(active)
+                s.step(nsteps)
+                for m in range(members):
+                    errs = compare(geom, o, s.get_state(m))
+                    assert max(errs.values()) <= TOL, (cands[i][0], active, m, errs)
+            s.set_active([*range(members)])
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_set_state_replaces_the_state(precision):
     """mcv_set_state (u, v, phi only) continues like mcv_set_member with the
