@@ -393,12 +393,23 @@ void launch_halo_batch(mcv_handle *const *hs, const int *curs, int count, int s,
   // z: grids' active members.  A block holds the segment's H + 1 lines.
   const int block = kHaloSeg * (hs[0]->H + 1);
   const dim3 grid((unsigned)((nmax + kHaloSeg - 1) / kHaloSeg), 24u, (unsigned)slots);
+  // programmatic stream serialization: the blocks may become resident during
+  // the stage kernel's last items and wait there (griddepcontrol.wait)
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(block);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   if (hs[0]->order == 3) {
-    if (mixed_inc) halo_kernel<3, true, NB><<<grid, block, 0, st>>>(b);
-    else halo_kernel<3, false, NB><<<grid, block, 0, st>>>(b);
+    if (mixed_inc) cudaLaunchKernelEx(&cfg, halo_kernel<3, true, NB>, b);
+    else cudaLaunchKernelEx(&cfg, halo_kernel<3, false, NB>, b);
   } else {
-    if (mixed_inc) halo_kernel<4, true, NB><<<grid, block, 0, st>>>(b);
-    else halo_kernel<4, false, NB><<<grid, block, 0, st>>>(b);
+    if (mixed_inc) cudaLaunchKernelEx(&cfg, halo_kernel<4, true, NB>, b);
+    else cudaLaunchKernelEx(&cfg, halo_kernel<4, false, NB>, b);
   }
 }
 

@@ -114,9 +114,6 @@ template <int D, bool MIXED, int NB>
 __global__ void __launch_bounds__(kHaloSeg * D) halo_kernel(const __grid_constant__ HaloBatch<NB> hb) {
   constexpr int H = D - 1;
   constexpr int NT = kHaloSeg * (H + 1);
-  // the next stage kernel may launch now: its items clear of the panel edges
-  // read nothing this kernel writes, the others wait for its completion
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   // the staged neighbour lines 1..H: {zonal, meridional, phi} on the sphere
   __shared__ double wz[H][kHaloWin], wm[H][kHaloWin], wp[H][kHaloWin];
   const int z = blockIdx.z;
@@ -210,6 +207,15 @@ __global__ void __launch_bounds__(kHaloSeg * D) halo_kernel(const __grid_constan
       cc = a.gcoef[(h - 1) * n + k];
     }
   }
+  // Launched with programmatic dependent launch, the blocks may be resident
+  // before the stage kernel that writes the increments, boundary copies and
+  // (FP64 form) the state has completed: everything above reads only what it
+  // leaves alone (the strip tables, the active list and, split precision, Y).
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // the next stage kernel may launch now (the stage kernel before this one
+  // has completed): its items clear of the panel edges read nothing this
+  // kernel writes, the others wait for its completion
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   // the boundary line (h = 0) needs no staged values
   bool store = live;

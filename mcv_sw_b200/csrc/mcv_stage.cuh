@@ -717,6 +717,9 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
     ty = item.ty;
     panel = item.panel;
     mem = IDENT ? item.slot : active_member(a.active, a.ident, item.slot);
+    // the CTA's last item: the halo kernel that follows may become resident
+    // (it waits for this grid's completion before reading what it writes)
+    if (wi + wstep >= wend) allow_dependent_launch();
   } else {
     // one CTA per (tile, panel, member) in panel order, which keeps the
     // neighbours' halo reads in L2; it starts once the previous kernel is done
