@@ -507,7 +507,7 @@ void number_items(StageBatch<NB> &b, int n) {
   b.total = nin + ned;
 }
 
-int launch_stage(mcv_handle *h, int cand, int s, int c) {
+int launch_stage(mcv_handle *h, int cand, int s, int c, bool pdl = true) {
   const StageLauncher &L = h->cands[cand];
   StageBatch<1> b;
   std::memset(&b, 0, sizeof(b));
@@ -516,11 +516,11 @@ int launch_stage(mcv_handle *h, int cand, int s, int c) {
   const int kind = stage_kind(h, s);
   const StageLaunchFn launch = h->active_ident ? L.launch_ident[kind] : L.launch[kind];
   if (!L.tma) {
-    launch(dim3(b.g[0].tiles_x * b.g[0].tiles_y, 6, h->n_active), h->stream, b);
+    launch(dim3(b.g[0].tiles_x * b.g[0].tiles_y, 6, h->n_active), h->stream, b, pdl);
     return MCV_OK;
   }
   const int ctas = std::max(1, std::min(b.total, h->bps[cand] * h->nsm));
-  launch(dim3(ctas), h->stream, b);
+  launch(dim3(ctas), h->stream, b, pdl);
   return MCV_OK;
 }
 
@@ -545,9 +545,10 @@ int autotune(mcv_handle *h) {
   int besti = 0;
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < h->ncands && e == cudaSuccess; ++i) {
-    int rc = launch_stage(h, i, 1, h->cur);  // warm-up
+    // plain launches: each starts after the previous one has completed
+    int rc = launch_stage(h, i, 1, h->cur, false);  // warm-up
     cudaEventRecord(e0, h->stream);
-    for (int r = 0; r < 3 && !rc; ++r) rc = launch_stage(h, i, 1, h->cur);
+    for (int r = 0; r < 3 && !rc; ++r) rc = launch_stage(h, i, 1, h->cur, false);
     if (rc) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
@@ -1628,7 +1629,7 @@ int enqueue_group_stage(mcv_group *g, const std::vector<mcv_handle *> &act, cons
     if (int rc = add_grid(b, (int)k, act[k], L, s, curs[k])) return rc;
   number_items(b, (int)act.size());
   const int ctas = std::max(1, std::min(b.total, g->bps * act[0]->nsm));
-  L.launch_batch[stage_kind(act[0], s)](dim3(ctas), g->stream, b);
+  L.launch_batch[stage_kind(act[0], s)](dim3(ctas), g->stream, b, true);
   launch_halo_batch<kMaxGrids>(act.data(), curs.data(), (int)act.size(), s, g->stream);
   return MCV_OK;
 }

@@ -1522,8 +1522,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
 // ---------------------------------------------------------------------------
 // Launch table of one tile shape (used by the tile-shape autotuner).
 // ---------------------------------------------------------------------------
-using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const StageBatch<1> &b);
-using StageBatchFn = void (*)(dim3 grid, cudaStream_t s, const StageBatch<kMaxGrids> &b);
+// pdl: launched with programmatic stream serialization (in a step, after a
+// halo kernel); the autotuner's back-to-back timing launches go without it
+using StageLaunchFn = void (*)(dim3 grid, cudaStream_t s, const StageBatch<1> &b, bool pdl);
+using StageBatchFn = void (*)(dim3 grid, cudaStream_t s, const StageBatch<kMaxGrids> &b, bool pdl);
 
 struct StageLauncher {
   int CX, CY, NT, minb;
@@ -1549,7 +1551,7 @@ struct StageConfig {
   // become resident while the preceding halo kernel finishes (TMA form: items
   // clear of the panel edges also run then; the rest wait for it)
   template <int KIND, int NB, bool IDENT = false>
-  static void launch_nb(dim3 grid, cudaStream_t s, const StageBatch<NB> &b) {
+  static void launch_nb(dim3 grid, cudaStream_t s, const StageBatch<NB> &b, bool pdl) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(NT);
@@ -1559,20 +1561,20 @@ struct StageConfig {
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = pdl ? 1 : 0;
     cudaLaunchKernelEx(&cfg, stage_kernel<D, CX, CY, NT, MINB, KIND, MIXED, WALK, TMA, OPT, NB, IDENT>, b);
   }
   template <int KIND>
-  static void launch(dim3 grid, cudaStream_t s, const StageBatch<1> &b) {
-    launch_nb<KIND, 1>(grid, s, b);
+  static void launch(dim3 grid, cudaStream_t s, const StageBatch<1> &b, bool pdl) {
+    launch_nb<KIND, 1>(grid, s, b, pdl);
   }
   template <int KIND>
-  static void launch_ident(dim3 grid, cudaStream_t s, const StageBatch<1> &b) {
-    launch_nb<KIND, 1, true>(grid, s, b);
+  static void launch_ident(dim3 grid, cudaStream_t s, const StageBatch<1> &b, bool pdl) {
+    launch_nb<KIND, 1, true>(grid, s, b, pdl);
   }
   template <int KIND>
-  static void launch_batch(dim3 grid, cudaStream_t s, const StageBatch<kMaxGrids> &b) {
-    if constexpr (TMA) launch_nb<KIND, kMaxGrids>(grid, s, b);
+  static void launch_batch(dim3 grid, cudaStream_t s, const StageBatch<kMaxGrids> &b, bool pdl) {
+    if constexpr (TMA) launch_nb<KIND, kMaxGrids>(grid, s, b, pdl);
   }
   template <int KIND>
   static cudaError_t attr() {
