@@ -370,10 +370,10 @@ __device__ __forceinline__ void cell_interior2(float2 o[D], const float2 *c, con
 
 // line_walk for two quantities at once (packed FP32 pairs, one eigenvalue per
 // interface): f and q point to the first point of the halo cell before the
-// walk, results go to outx (first of the pair) and outy (second).
+// walk, the result pairs go to out.
 template <int D, int NMAX, int S, int OS, class L>
 __device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, const L &lam, int ncells, bool ends,
-                                           float *outx, float *outy, const Widths<float> &w) {
+                                           float2 *out, const Widths<float> &w) {
   const float2 ip = bc2((D == 3) ? w.inv_dx : w.inv_2dx);
   float2 cf[D], cq[D];
 #pragma unroll
@@ -409,14 +409,8 @@ __device__ __forceinline__ void line_walk2(const float2 *f, const float2 *q, con
       o[D - 1] = fluxR;
       cell_interior2<D, 1>(o, cf, w);
 #pragma unroll
-      for (int m = 0; m < D - 1; ++m) {
-        outx[(c * (D - 1) + m) * OS] = o[m].x;
-        outy[(c * (D - 1) + m) * OS] = o[m].y;
-      }
-      if (c == ncells - 1 && ends) {
-        outx[(c * (D - 1) + D - 1) * OS] = o[D - 1].x;
-        outy[(c * (D - 1) + D - 1) * OS] = o[D - 1].y;
-      }
+      for (int m = 0; m < D - 1; ++m) out[(c * (D - 1) + m) * OS] = o[m];
+      if (c == ncells - 1 && ends) out[(c * (D - 1) + D - 1) * OS] = o[D - 1];
 #pragma unroll
       for (int m = 0; m < D; ++m) {
         cf[m] = nf[m];
@@ -459,9 +453,10 @@ struct Tile {
   static constexpr int LAMY = SGNX + TY * (CX + 1);  // [TX][CY+1]
   static constexpr int SGNY = LAMY + TX * (CY + 1);
   static constexpr int GPX = LAMX, GPY = LAMX + I;  // split precision [TY][TX] each
-  // ... sweep results [3][TY][TX] each ...
+  // ... sweep results [3][TY][TX] each (split precision: the first two as
+  // float2 pairs [TY][TX] {flux, divergence}, then the third) ...
   static constexpr int XR = PAIRED ? GPY + I : SGNY + TX * (CY + 1);
-  static constexpr int YR = XR + 3 * I;
+  static constexpr int YR = XR + 3 * I + (PAIRED ? (I & 1) : 0);  // float2-aligned
   static constexpr int TOTAL = YR + 3 * I;
   // split precision, after the R arrays: 1-D metric tables [LX] and [LY] double4,
   // then two buffers (alternate work items of the TMA form) of the per-tile
@@ -490,6 +485,7 @@ struct Tile {
   __host__ __device__ static constexpr size_t bar_off(bool mixed) { return field_off(mixed, mixed ? 7 : 8); }
   __host__ __device__ static constexpr size_t bytes_tma(bool mixed) { return bar_off(mixed) + 16; }
   static_assert(LX % 2 == 1, "odd shared row length");
+  static_assert(!PAIRED || (XR % 2 == 0 && YR % 2 == 0), "float2 sweep results");
 };
 
 // Split precision: the FP64 quantities of one loaded point.  q = {E - phibar,
@@ -1120,16 +1116,16 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         const int r = it % T::TY, c0 = (it / T::TY) * S0X;
         if (r >= tye || c0 >= ncx) continue;
         const int w0 = (r + H) * LX + c0 * (D - 1);
-        R *xr = sm + T::XR + r * T::TX + c0 * (D - 1);
+        float2 *xp = reinterpret_cast<float2 *>(sm + T::XR) + r * T::TX + c0 * (D - 1);
         line_walk2<D, S0X, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, EigLam{sm + T::CU + r * T::TX + c0 * (D - 1), sm + T::GPX + r * T::TX + c0 * (D - 1), D - 1},
-                                 min(S0X, ncx - c0), c0 + S0X >= ncx, xr, xr + T::I, w);
+                                 min(S0X, ncx - c0), c0 + S0X >= ncx, xp, w);
       } else if (it < E0Y) {
         const int j = it - E0X, q = j % T::TX, c0 = (j / T::TX) * S0Y;
         if (q >= txe || c0 >= ncy) continue;
         const int w0 = c0 * (D - 1) * LX + (q + H);
-        R *yr = sm + T::YR + q + c0 * (D - 1) * T::TX;
+        float2 *yp = reinterpret_cast<float2 *>(sm + T::YR) + q + c0 * (D - 1) * T::TX;
         line_walk2<D, S0Y, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, EigLam{sm + T::CV + c0 * (D - 1) * T::TX + q, sm + T::GPY + c0 * (D - 1) * T::TX + q, (D - 1) * T::TX},
-                                      min(S0Y, ncy - c0), c0 + S0Y >= ncy, yr, yr + T::I, w);
+                                      min(S0Y, ncy - c0), c0 + S0Y >= ncy, yp, w);
       } else if (it < E1X) {
         const int j = it - E0Y, r = j % T::TY, c0 = (j / T::TY) * S1X;
         if (r >= tye || c0 >= ncx) continue;
@@ -1165,7 +1161,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         R *xr = sm + T::XR + r * T::TX + c0 * (D - 1);
         if (kk == 0)
           line_walk2<D, SEGX, 1, 1>(s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, EigLam{sm + T::CU + r * T::TX + c0 * (D - 1), sm + T::GPX + r * T::TX + c0 * (D - 1), D - 1}, nseg,
-                                    ends, xr, xr + T::I, w);
+                                    ends, reinterpret_cast<float2 *>(sm + T::XR) + r * T::TX + c0 * (D - 1), w);
         else
           line_walk<D, SEGX, 1, 1, true, R>(sm + T::V + w0, sm + T::V + w0, SgnLam{sm + T::CU + r * T::TX + c0 * (D - 1), D - 1}, nseg,
                                             ends, xr + 2 * T::I, w);
@@ -1180,7 +1176,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         R *yr = sm + T::YR + q + c0 * (D - 1) * T::TX;
         if (kk == 0)
           line_walk2<D, SEGY, LX, T::TX>(s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, EigLam{sm + T::CV + c0 * (D - 1) * T::TX + q, sm + T::GPY + c0 * (D - 1) * T::TX + q, (D - 1) * T::TX},
-                                         nseg, ends, yr, yr + T::I, w);
+                                         nseg, ends, reinterpret_cast<float2 *>(sm + T::YR) + q + c0 * (D - 1) * T::TX, w);
         else
           line_walk<D, SEGY, LX, T::TX, true, R>(sm + T::U + w0, sm + T::U + w0, SgnLam{sm + T::CV + c0 * (D - 1) * T::TX + q, (D - 1) * T::TX},
                                                  nseg, ends, yr + 2 * T::I, w);
@@ -1203,12 +1199,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         float2 d[D];
         const EigLam lam{sm + T::CU + r * T::TX + c * (D - 1), sm + T::GPX + r * T::TX + c * (D - 1), D - 1};
         cell_derivs2<D, 1>(d, s2 + T::XF / 2 + w0, s2 + T::XQ / 2 + w0, lam(0), lam(1), w);
+        float2 *xp = reinterpret_cast<float2 *>(sm + T::XR) + r * T::TX + c * (D - 1);
 #pragma unroll
         for (int m = 0; m < D; ++m)
-          if (m < mmax) {
-            xr[m] = d[m].x;
-            xr[T::I + m] = d[m].y;
-          }
+          if (m < mmax) xp[m] = d[m];
       } else {
         R d[D];
         const SgnLam sgn{sm + T::CU + r * T::TX + c * (D - 1), D - 1};
@@ -1231,12 +1225,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         float2 d[D];
         const EigLam lam{sm + T::CV + c * (D - 1) * T::TX + q, sm + T::GPY + c * (D - 1) * T::TX + q, (D - 1) * T::TX};
         cell_derivs2<D, LX>(d, s2 + T::YF / 2 + w0, s2 + T::YQ / 2 + w0, lam(0), lam(1), w);
+        float2 *yp = reinterpret_cast<float2 *>(sm + T::YR) + (c * (D - 1)) * T::TX + q;
 #pragma unroll
         for (int m = 0; m < D; ++m)
-          if (m < mmax) {
-            yr[m * T::TX] = d[m].x;
-            yr[T::I + m * T::TX] = d[m].y;
-          }
+          if (m < mmax) yp[m * T::TX] = d[m];
       } else {
         R d[D];
         const SgnLam sgn{sm + T::CV + c * (D - 1) * T::TX + q, (D - 1) * T::TX};
@@ -1345,6 +1337,15 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
   // base, accumulators, input increments, Coriolis), so their latencies
   // overlap, then assembles and stores them.
   constexpr int CHA = 2;
+  // split precision: the linear references' exact derivatives (E and v along
+  // x, E and u along y), the same for every point of the item
+  float sl[4] = {0.f, 0.f, 0.f, 0.f};
+  if constexpr (MIXED) {
+    sl[0] = slope[0];
+    sl[1] = slope[2];
+    sl[2] = slope[3 + 0];
+    sl[3] = slope[3 + 1];
+  }
   constexpr bool NEED_BASE = MIXED ? last_stage(KIND) : !first_stage(KIND);
   constexpr bool NEED_ACC = (KIND == RK4_S2 || KIND == RK4_S3 || KIND == RK4_S4);
   constexpr bool NEED_INC = MIXED && (KIND == RK3_S2 || KIND == RK3_S3);
@@ -1398,15 +1399,27 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
     const R sg = sm[T::SG + it], cu = sm[T::CU + it], cv = sm[T::CV + it];
     const R fc = MIXED ? sm[T::FC + it] : (R)gf[k];
     const R rsg = MIXED ? sg : R(1) / sg;
-    R flux_x = sm[T::XR + it], dvdx = sm[T::XR + 2 * T::I + it];
-    R flux_y = sm[T::YR + it], dudy = sm[T::YR + 2 * T::I + it];
-    const R div_x = sm[T::XR + T::I + it], div_y = sm[T::YR + T::I + it];
+    R flux_x, div_x, flux_y, div_y;
+    if constexpr (MIXED) {
+      const float2 px = reinterpret_cast<const float2 *>(sm + T::XR)[it];
+      const float2 py = reinterpret_cast<const float2 *>(sm + T::YR)[it];
+      flux_x = px.x;
+      div_x = px.y;
+      flux_y = py.x;
+      div_y = py.y;
+    } else {
+      flux_x = sm[T::XR + it];
+      div_x = sm[T::XR + T::I + it];
+      flux_y = sm[T::YR + it];
+      div_y = sm[T::YR + T::I + it];
+    }
+    R dvdx = sm[T::XR + 2 * T::I + it], dudy = sm[T::YR + 2 * T::I + it];
     if constexpr (MIXED) {
       // the linear references' exact derivatives: E and v along x, E and u along y
-      flux_x += slope[0];
-      dvdx += slope[2];
-      flux_y += slope[3 + 0];
-      dudy += slope[3 + 1];
+      flux_x += sl[0];
+      dvdx += sl[1];
+      flux_y += sl[2];
+      dudy += sl[3];
     }
     const R tP = -div_x - div_y;
     R tU, tV;
