@@ -494,7 +494,8 @@ def run_ours(args):
     # (relative, pointwise): the twin shows how far the flow itself amplifies a
     # perturbation of that size
     accuracy = None
-    if rank == 0 and args.error_days > 0:
+    # (one GPU only: at N > 1 the other ranks would wait for it at the final barrier)
+    if rank == 0 and world == 1 and args.error_days > 0:
         nsteps = int(round(args.error_days * 86400.0 / st.dt))
         twin_phi = st.phi * (1.0 + 1e-12 * np.random.default_rng(0).standard_normal(st.phi.shape))
         runs = {"fp64": ("fp64", st.phi), "fp64_twin": ("fp64", twin_phi), "mixed": ("mixed", st.phi)}
