@@ -92,7 +92,8 @@ struct HaloBatch {
 // Positions along an edge per block, and the window of neighbour positions a
 // block stages per halo line.  The interpolation stencil of the ghost point at
 // position k starts at neighbour position (iref - 1)(D - 1), within [k - 6,
-// k + 2] on every line at every Nc of the equiangular grids, so the window
+// k + 2] on every line of the equiangular grids (checked for Nc = 8 to 1024,
+// both orders), so the window
 // [k0 - kHaloLead, k0 - kHaloLead + kHaloWin) of a segment starting at k0
 // holds all of its stencils without reading iref first; a stencil point
 // outside the window is read from global memory instead.
